@@ -1,0 +1,156 @@
+/* spectral.h -- C ABI of the B200 spectral path-tracing library (libspectral.so).
+ *
+ * Drop-in for the Taichi kernels and module-global fields of
+ * Xyzonox/taichi-spectral-render main.py.  Every entry point names the
+ * reference code it replaces.  Conventions:
+ *   - every call returns ts_status; on failure ts_last_error() describes it;
+ *   - device pointers are CUDA device addresses on the context's device;
+ *     "stream" is a cudaStream_t (NULL = the legacy default stream); calls are
+ *     stream-ordered and a context must not be used from two threads at once;
+ *   - scene arrays are caller-owned host memory, copied during the call;
+ *   - pixel (i, j): i is the column (0..width-1), j the row counted from the
+ *     bottom, as the reference indexes pixels_geometry[i, j] (main.py:1505).
+ */
+#ifndef TS_SPECTRAL_H
+#define TS_SPECTRAL_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ts_ctx ts_ctx;
+
+typedef enum {
+  TS_OK = 0,
+  TS_ERR_INVALID_ARG = 1,
+  TS_ERR_CUDA = 2,
+  TS_ERR_OUT_OF_MEMORY = 3,
+  TS_ERR_CAPACITY = 4,      /* a queue or table bound was exceeded */
+  TS_ERR_DEVICE_FAULT = 5,  /* a kernel reported an error bit (stack overflow, iteration cap) */
+  TS_ERR_NO_SCENE = 6
+} ts_status;
+
+/* Render kernels */
+enum { TS_KERNEL_MEGA = 0, TS_KERNEL_WAVEFRONT = 1 };
+/* Traversal modes of ts_trace_batch */
+enum { TS_TRACE_FAST = 0, TS_TRACE_REFERENCE_ORDER = 1 };
+/* Film buffers */
+enum { TS_FILM_BLOCK = 0, TS_FILM_MEAN = 1, TS_FILM_M2 = 2 };
+
+/* Render constants of main.py:11-35 as runtime values. */
+typedef struct {
+  int32_t width, height;         /* RENDER_WIDTH, RENDER_HEIGHT */
+  int32_t bands;                 /* SPECTRAL_BANDS (1..64) */
+  float lambda_min_nm, lambda_max_nm; /* WAVELENGTH_MIN, WAVELENGTH_MAX */
+  int32_t max_path_length;       /* MAX_PATH_LENGTH */
+  int32_t scatter_bounces;       /* SCATTER_BOUNCES (shadow segments) */
+  float epsilon, escape;         /* EPSILON, ESCAPE */
+  float aspect_ratio;            /* ASPECT_RATIO */
+  float fov_scale;               /* 1.0 = the reference's fixed half-FOV atan(1/2); s gives atan(s/2) */
+  uint32_t seed;                 /* Philox key word 0 (word 1 is the pass index) */
+  uint32_t scene_id;             /* Philox counter word 2 (distinguishes scenes of a batch) */
+  int32_t device;                /* CUDA device ordinal */
+  int32_t kernel;                /* TS_KERNEL_MEGA or TS_KERNEL_WAVEFRONT */
+  int32_t block_size;            /* threads per block of the render kernels (0 = default) */
+  int32_t blocks_per_sm;         /* persistent grid = SMs * blocks_per_sm (0 = default) */
+  int32_t sort_keys;             /* wavefront: sort shading queue by material (0 = off) */
+} ts_config;
+
+/* Scene in the reference's data model (setup_scene, main.py:509-631). Triangles
+ * are given in ORIGINAL order; the library reorders them into BVH order. */
+typedef struct {
+  int32_t num_tris;
+  const float *v0, *v1, *v2;        /* [T][3] vertices */
+  const float *n0, *n1, *n2;        /* [T][3] vertex normals (the face normal where the mesh has none) */
+  const float *normal;              /* [T][3] unit geometric normal, as main.py:525-534 computes it */
+  const float *area;                /* [T] triangle area */
+  const int32_t *mat_id;            /* [T] */
+  int32_t num_materials;
+  const float *mat_f32;             /* [M][6][B]: n, k, roughness, scattering, emission, anisotropy */
+  const int32_t *mat_i32;           /* [M][2][B]: is_true_volume, surface_emission */
+  const int32_t *mat_eem;           /* [M]: EEM id (0 = none) */
+  int32_t num_eems;                 /* rows of eem, including the unused id 0 */
+  const float *eem;                 /* [E][B][B], row = excitation band (may be NULL if num_eems == 0) */
+  const float *cmf;                 /* [B][3] colour-matching functions at the band centres */
+  /* BVH: bvh_num_nodes == 0 builds one (binned SAH); otherwise the tree is
+   * adopted as given in the reference layout (main.py:267-275, e.g. the
+   * output of the reference's build_bvh), with tri_perm[slot] = original index. */
+  int32_t bvh_num_nodes;
+  const float *node_min, *node_max; /* [N][3] */
+  const int32_t *node_left, *node_right, *node_num_tris, *node_tri_start, *tri_perm;
+  /* binned-SAH parameters (0 = defaults) */
+  int32_t bvh_bins, bvh_leaf_max;
+  float bvh_cost_trav, bvh_cost_tri;
+} ts_scene_desc;
+
+typedef struct {
+  int32_t num_tris, num_nodes, num_ref_nodes, max_depth, leaves;
+  double sah_cost;
+  int32_t max_lights;
+  size_t device_bytes;  /* device memory held by the context */
+} ts_scene_info;
+
+/* ---- context (replaces ti.init + the module-global fields, main.py:9, 361-394) */
+ts_status ts_create(const ts_config *cfg, ts_ctx **out);
+ts_status ts_destroy(ts_ctx *ctx);
+const char *ts_last_error(const ts_ctx *ctx); /* ctx may be NULL: last error of this thread */
+const char *ts_version(void);
+
+/* ---- scene (setup_scene + build_bvh + get_scene_dimensions, main.py:398-631) */
+ts_status ts_upload_scene(ts_ctx *ctx, const ts_scene_desc *scene);
+ts_status ts_scene_info_get(const ts_ctx *ctx, ts_scene_info *info);
+/* slot -> original triangle index, [num_tris] host array */
+ts_status ts_get_tri_perm(const ts_ctx *ctx, int32_t *perm_out);
+
+/* Host-only BVH build (replaces build_bvh, main.py:437-507): the binned-SAH
+ * tree ts_upload_scene would build, returned in the reference layout.
+ * Output arrays hold max_nodes entries (2*num_tris-1 always suffices);
+ * tri_perm[slot] = original triangle index.  Needs no GPU. */
+ts_status ts_build_bvh_host(int32_t num_tris, const float *v0, const float *v1, const float *v2, int32_t bins,
+                            int32_t leaf_max, float cost_trav, float cost_tri, int32_t max_nodes, float *node_min,
+                            float *node_max, int32_t *node_left, int32_t *node_right, int32_t *node_num_tris,
+                            int32_t *node_tri_start, int32_t *tri_perm, int32_t *num_nodes_out);
+
+/* ---- camera (update_camera, main.py:633-640) */
+ts_status ts_set_camera(ts_ctx *ctx, const float origin[3], const float lookat[3], const float up[3]);
+
+/* ---- render (cast_rays(current_sample_in_block, block_index), main.py:1502-1590).
+ * pass_idx selects the random stream (Philox key word 1); band is the pass's
+ * wavelength index (current_sample_in_block).  Deposits into TS_FILM_BLOCK. */
+ts_status ts_render_pass(ts_ctx *ctx, uint32_t pass_idx, int32_t band, void *stream);
+
+/* ---- film (average_and_reset_block, clear_pixel_space, main.py:1592-1607, 1661-1674) */
+ts_status ts_accumulate_block(ts_ctx *ctx, int32_t num_blocks_completed, void *stream);
+ts_status ts_reset(ts_ctx *ctx, void *stream);
+/* device pointer + element count of a film buffer ([B][H][W] float64) */
+ts_status ts_film_buffer(ts_ctx *ctx, int32_t which, double **dev_ptr, size_t *count);
+/* copy a film buffer to host memory (synchronises the stream) */
+ts_status ts_film_download(ts_ctx *ctx, int32_t which, double *host, void *stream);
+
+/* ---- resolve (color_rays, main.py:1609-1629).  scale multiplies the CMF dot
+ * product: WAVELENGTH_STEP / normalization_factor in the reference.
+ * xyz_dev: [H][W][3] float32 device buffer. */
+ts_status ts_resolve_xyz(ts_ctx *ctx, double scale, float *xyz_dev, void *stream);
+/* same, into a host buffer (device scratch, copy back, stream synchronised) */
+ts_status ts_resolve_xyz_host(ts_ctx *ctx, double scale, float *xyz_host, void *stream);
+/* full color_rays: upscale to img_w x img_h, XYZ->RGB (row-major 3x3), Reinhard, gamma. */
+ts_status ts_resolve_rgb(ts_ctx *ctx, double scale, const float xyz_to_rgb[9], float exposure, float gamma,
+                         int32_t img_w, int32_t img_h, float *rgb_dev, void *stream);
+
+/* ---- geometry (trace, main.py:831-864; visualize_normals, main.py:1631-1659) */
+/* rays_dev: [n][6] (origin, direction); outputs [n] device arrays, tri = original
+ * triangle index or -1, t = 1e9 on a miss; u/v may be NULL. */
+ts_status ts_trace_batch(ts_ctx *ctx, const float *rays_dev, int32_t n, int32_t mode, int32_t *tri_dev,
+                         float *t_dev, float *u_dev, float *v_dev, void *stream);
+/* normals_dev: [H][W][3] float32 */
+ts_status ts_render_normals(ts_ctx *ctx, float *normals_dev, void *stream);
+
+/* ---- device status: error bits raised by kernels since the last call (synchronises) */
+ts_status ts_check_device(ts_ctx *ctx, uint32_t *bits);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TS_SPECTRAL_H */

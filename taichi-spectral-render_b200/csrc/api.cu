@@ -1,0 +1,598 @@
+// C ABI of libspectral.so (include/spectral.h): context, scene upload, render
+// passes, film operations.  The context owns every device buffer; callers pass
+// plain pointers and sizes.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "bvh.h"
+#include "kernels.cuh"
+#include "spectral.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+constexpr int kMaxBands = 64;
+
+}  // namespace
+
+struct ts_ctx {
+  ts_config cfg{};
+  ts::DevConfig dc{};
+  int num_sms = 0;
+  bool has_scene = false;
+  ts::DevScene ds{};
+  std::vector<void *> scene_allocs;
+  std::vector<int32_t> perm;
+  ts_scene_info info{};
+  float *d_cmf = nullptr;
+  double *d_film[3] = {nullptr, nullptr, nullptr};
+  int *d_counter = nullptr;
+  uint32_t *d_err = nullptr;
+  float *d_xyz = nullptr;
+  float *d_m9 = nullptr;  // XYZ->RGB matrix for ts_resolve_rgb
+  ts::WaveBuffers wave{};
+  std::vector<void *> wave_allocs;
+  size_t film_bytes = 0, scene_bytes = 0, wave_bytes = 0;
+  float cam[9] = {0, 0, 3.5f, 0, 0, -1, 0, 1, 0};
+  std::string err;
+};
+
+namespace {
+
+ts_status fail(ts_ctx *c, ts_status s, const std::string &msg) {
+  g_last_error = msg;
+  if (c) c->err = msg;
+  return s;
+}
+ts_status cuda_fail(ts_ctx *c, cudaError_t e, const char *what) {
+  return fail(c, e == cudaErrorMemoryAllocation ? TS_ERR_OUT_OF_MEMORY : TS_ERR_CUDA,
+              std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define TS_CUDA(c, expr, what)                       \
+  do {                                               \
+    cudaError_t e_ = (expr);                         \
+    if (e_ != cudaSuccess) return cuda_fail(c, e_, what); \
+  } while (0)
+
+cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+ts::Film film_of(ts_ctx *c) {
+  ts::Film f;
+  f.block = c->d_film[TS_FILM_BLOCK];
+  f.mean = c->d_film[TS_FILM_MEAN];
+  f.m2 = c->d_film[TS_FILM_M2];
+  f.W = c->cfg.width;
+  f.H = c->cfg.height;
+  f.B = c->cfg.bands;
+  return f;
+}
+
+void free_list(std::vector<void *> &v) {
+  for (void *p : v) cudaFree(p);
+  v.clear();
+}
+
+template <class T>
+cudaError_t upload(ts_ctx *c, std::vector<void *> &owner, const T *host, size_t n, T **dev, size_t &bytes) {
+  *dev = nullptr;
+  const size_t sz = std::max<size_t>(n, 1) * sizeof(T);
+  cudaError_t e = cudaMalloc((void **)dev, sz);
+  if (e != cudaSuccess) return e;
+  owner.push_back(*dev);
+  bytes += sz;
+  if (n) e = cudaMemcpy(*dev, host, n * sizeof(T), cudaMemcpyHostToDevice);
+  return e;
+}
+
+void camera_basis(const float o[3], const float l[3], const float up[3], float3 &w, float3 &u, float3 &v) {
+  // update_camera, main.py:633-640, in float32
+  auto norm = [](float3 a) {
+    const float n = std::sqrt(a.x * a.x + a.y * a.y + a.z * a.z);
+    return make_float3(a.x / n, a.y / n, a.z / n);
+  };
+  auto cr = [](float3 a, float3 b) {
+    return make_float3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+  };
+  w = norm(make_float3(o[0] - l[0], o[1] - l[1], o[2] - l[2]));
+  u = norm(cr(make_float3(up[0], up[1], up[2]), w));
+  v = cr(w, u);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *ts_version(void) { return "spectral-b200 0.1 (sm_100a)"; }
+
+const char *ts_last_error(const ts_ctx *ctx) { return ctx ? ctx->err.c_str() : g_last_error.c_str(); }
+
+ts_status ts_create(const ts_config *cfg, ts_ctx **out) {
+  if (!cfg || !out) return fail(nullptr, TS_ERR_INVALID_ARG, "ts_create: null argument");
+  *out = nullptr;
+  const ts_config &k = *cfg;
+  if (k.width <= 0 || k.height <= 0 || (int64_t)k.width * k.height > (1ll << 30))
+    return fail(nullptr, TS_ERR_INVALID_ARG, "ts_create: resolution out of range");
+  if (k.bands < 1 || k.bands > kMaxBands) return fail(nullptr, TS_ERR_INVALID_ARG, "ts_create: bands must be 1..64");
+  if (k.max_path_length < 0 || k.max_path_length > 1024)
+    return fail(nullptr, TS_ERR_INVALID_ARG, "ts_create: max_path_length must be 0..1024");
+  if (k.scatter_bounces < 1 || k.scatter_bounces > 64)
+    return fail(nullptr, TS_ERR_INVALID_ARG, "ts_create: scatter_bounces must be 1..64");
+  if (k.bands > 1 && !(k.lambda_max_nm > k.lambda_min_nm))
+    return fail(nullptr, TS_ERR_INVALID_ARG, "ts_create: lambda_max_nm must exceed lambda_min_nm");
+  if (k.kernel != TS_KERNEL_MEGA && k.kernel != TS_KERNEL_WAVEFRONT)
+    return fail(nullptr, TS_ERR_INVALID_ARG, "ts_create: unknown kernel");
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) return fail(nullptr, TS_ERR_CUDA, "ts_create: no CUDA device");
+  if (k.device < 0 || k.device >= ndev) return fail(nullptr, TS_ERR_INVALID_ARG, "ts_create: bad device ordinal");
+  e = cudaSetDevice(k.device);
+  if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaSetDevice");
+  ts_ctx *c = new ts_ctx();
+  c->cfg = k;
+  if (c->cfg.block_size <= 0) c->cfg.block_size = 128;
+  c->cfg.block_size = std::min(1024, std::max(32, c->cfg.block_size / 32 * 32));
+  cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, k.device);
+  ts::DevConfig &d = c->dc;
+  d.W = k.width;
+  d.H = k.height;
+  d.B = k.bands;
+  d.lmin_m = (float)((double)k.lambda_min_nm * 1e-9);
+  d.lmin_nm = k.lambda_min_nm;
+  d.step_nm = k.bands > 1 ? (float)(((double)k.lambda_max_nm - (double)k.lambda_min_nm) / (k.bands - 1)) : 0.f;
+  d.eps = k.epsilon;
+  d.escape = k.escape;
+  d.max_depth = k.max_path_length;
+  d.scatter_bounces = k.scatter_bounces;
+  d.aspect = k.aspect_ratio;
+  d.fov = k.fov_scale;
+  d.seed = k.seed;
+  d.scene_id = k.scene_id;
+  const size_t cells = (size_t)k.width * k.height * k.bands;
+  for (int i = 0; i < 3; ++i) {
+    e = cudaMalloc((void **)&c->d_film[i], cells * sizeof(double));
+    if (e != cudaSuccess) {
+      ts_destroy(c);
+      return cuda_fail(nullptr, e, "ts_create: film allocation");
+    }
+    cudaMemset(c->d_film[i], 0, cells * sizeof(double));
+  }
+  c->film_bytes = 3 * cells * sizeof(double);
+  e = cudaMalloc((void **)&c->d_counter, 64 * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_err, sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_xyz, (size_t)k.width * k.height * 3 * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_m9, 9 * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemset(c->d_err, 0, sizeof(uint32_t));
+  if (e != cudaSuccess) {
+    ts_destroy(c);
+    return cuda_fail(nullptr, e, "ts_create: allocation");
+  }
+  *out = c;
+  return TS_OK;
+}
+
+ts_status ts_destroy(ts_ctx *c) {
+  if (!c) return TS_OK;
+  cudaSetDevice(c->cfg.device);
+  free_list(c->scene_allocs);
+  free_list(c->wave_allocs);
+  for (double *p : c->d_film) cudaFree(p);
+  cudaFree(c->d_counter);
+  cudaFree(c->d_err);
+  cudaFree(c->d_xyz);
+  cudaFree(c->d_m9);
+  delete c;
+  return TS_OK;
+}
+
+ts_status ts_upload_scene(ts_ctx *c, const ts_scene_desc *sd) {
+  if (!c || !sd) return fail(c, TS_ERR_INVALID_ARG, "ts_upload_scene: null argument");
+  cudaSetDevice(c->cfg.device);
+  const int T = sd->num_tris, M = sd->num_materials, B = c->cfg.bands, E = sd->num_eems;
+  if (T < 0 || (T > 0 && (!sd->v0 || !sd->v1 || !sd->v2 || !sd->n0 || !sd->n1 || !sd->n2 || !sd->normal ||
+                          !sd->area || !sd->mat_id)))
+    return fail(c, TS_ERR_INVALID_ARG, "ts_upload_scene: missing triangle arrays");
+  if (M <= 0 || !sd->mat_f32 || !sd->mat_i32 || !sd->mat_eem)
+    return fail(c, TS_ERR_INVALID_ARG, "ts_upload_scene: at least one material (air, id 0) is required");
+  if (E < 0 || (E > 0 && !sd->eem)) return fail(c, TS_ERR_INVALID_ARG, "ts_upload_scene: missing EEM table");
+  if (!sd->cmf) return fail(c, TS_ERR_INVALID_ARG, "ts_upload_scene: missing CMF table");
+  for (int t = 0; t < T; ++t)
+    if (sd->mat_id[t] < 0 || sd->mat_id[t] >= M)
+      return fail(c, TS_ERR_INVALID_ARG, "ts_upload_scene: triangle " + std::to_string(t) + " has material id " +
+                                             std::to_string(sd->mat_id[t]) + " outside 0.." +
+                                             std::to_string(M - 1));
+  for (int m = 0; m < M; ++m)
+    if (sd->mat_eem[m] < 0 || (sd->mat_eem[m] > 0 && sd->mat_eem[m] >= E))
+      return fail(c, TS_ERR_INVALID_ARG, "ts_upload_scene: material " + std::to_string(m) + " names EEM " +
+                                             std::to_string(sd->mat_eem[m]) + " but only " + std::to_string(E) +
+                                             " EEM rows were given");
+  for (size_t i = 0; i < (size_t)9 * T; ++i) {
+    const float x = (i < (size_t)3 * T ? sd->v0 : (i < (size_t)6 * T ? sd->v1 : sd->v2))[i % (3 * (size_t)T)];
+    if (!std::isfinite(x)) return fail(c, TS_ERR_INVALID_ARG, "ts_upload_scene: non-finite vertex coordinate");
+  }
+
+  // ---- BVH
+  ts::BvhOut bvh;
+  std::string err;
+  if (sd->bvh_num_nodes > 0) {
+    if (!sd->node_min || !sd->node_max || !sd->node_left || !sd->node_right || !sd->node_num_tris ||
+        !sd->node_tri_start || !sd->tri_perm)
+      return fail(c, TS_ERR_INVALID_ARG, "ts_upload_scene: incomplete reference BVH");
+    if (!ts::bvh_from_reference(T, sd->v0, sd->v1, sd->v2, sd->bvh_num_nodes, sd->node_min, sd->node_max,
+                                sd->node_left, sd->node_right, sd->node_num_tris, sd->node_tri_start, sd->tri_perm,
+                                bvh, err))
+      return fail(c, TS_ERR_INVALID_ARG, "ts_upload_scene: " + err);
+  } else {
+    ts::BvhParams p;
+    if (sd->bvh_bins > 0) p.bins = sd->bvh_bins;
+    if (sd->bvh_leaf_max > 0) p.leaf_max = std::min(sd->bvh_leaf_max, ts::kLeafMax);
+    if (sd->bvh_cost_trav > 0) p.cost_trav = sd->bvh_cost_trav;
+    if (sd->bvh_cost_tri > 0) p.cost_tri = sd->bvh_cost_tri;
+    if (!ts::build_bvh_binned(T, sd->v0, sd->v1, sd->v2, p, bvh, err))
+      return fail(c, TS_ERR_INVALID_ARG, "ts_upload_scene: " + err);
+  }
+
+  // ---- triangles in slot order
+  std::vector<float4> tri((size_t)3 * T), shade((size_t)3 * T);
+  std::vector<int32_t> slot_mat(T);
+  for (int s = 0; s < T; ++s) {
+    const int o = bvh.perm[s];
+    const float *a = sd->v0 + 3 * (size_t)o, *b = sd->v1 + 3 * (size_t)o, *q = sd->v2 + 3 * (size_t)o;
+    int32_t oid = o, mid = sd->mat_id[o];
+    float fo, fm;
+    std::memcpy(&fo, &oid, 4);
+    std::memcpy(&fm, &mid, 4);
+    tri[3 * s + 0] = make_float4(a[0], a[1], a[2], fo);
+    tri[3 * s + 1] = make_float4(b[0] - a[0], b[1] - a[1], b[2] - a[2], fm);
+    tri[3 * s + 2] = make_float4(q[0] - a[0], q[1] - a[1], q[2] - a[2], 0.f);
+    const float *g = sd->normal + 3 * (size_t)o;
+    const float *n0 = sd->n0 + 3 * (size_t)o, *n1 = sd->n1 + 3 * (size_t)o, *n2 = sd->n2 + 3 * (size_t)o;
+    shade[3 * s + 0] = make_float4(n0[0], n0[1], n0[2], g[0]);
+    shade[3 * s + 1] = make_float4(n1[0], n1[1], n1[2], g[1]);
+    shade[3 * s + 2] = make_float4(n2[0], n2[1], n2[2], g[2]);
+    slot_mat[s] = mid;
+  }
+  // ---- materials, main.py:545-561
+  std::vector<float4> mat((size_t)M * B * 2);
+  for (int m = 0; m < M; ++m)
+    for (int b = 0; b < B; ++b) {
+      const float *f = sd->mat_f32 + (size_t)m * 6 * B;
+      const int32_t *i = sd->mat_i32 + (size_t)m * 2 * B;
+      float iv, se;
+      std::memcpy(&iv, &i[0 * B + b], 4);
+      std::memcpy(&se, &i[1 * B + b], 4);
+      mat[((size_t)m * B + b) * 2 + 0] = make_float4(f[0 * B + b], f[1 * B + b], f[2 * B + b], f[3 * B + b]);
+      mat[((size_t)m * B + b) * 2 + 1] = make_float4(f[4 * B + b], f[5 * B + b], iv, se);
+    }
+  // ---- EEM tables: row maximum (quantum yield) and running CDF, float32 in
+  // the order the reference's kernels accumulate them (main.py:1247-1272)
+  const int Ee = std::max(E, 1);
+  std::vector<float> eem((size_t)Ee * B * B, 0.f), qy((size_t)Ee * B, 0.f), cdf((size_t)Ee * B * B, 0.f);
+  if (E > 0) std::memcpy(eem.data(), sd->eem, sizeof(float) * (size_t)E * B * B);
+  for (int e = 0; e < E; ++e)
+    for (int r = 0; r < B; ++r) {
+      const float *row = eem.data() + ((size_t)e * B + r) * B;
+      float q = 0.f, norm = 0.f;
+      for (int j = 0; j < B; ++j) {
+        if (row[j] > q) q = row[j];
+        norm += row[j];
+      }
+      qy[(size_t)e * B + r] = q;
+      float cum = 0.f;
+      for (int j = 0; j < B; ++j) {
+        cum += row[j] / norm;
+        cdf[((size_t)e * B + r) * B + j] = norm != 0.f ? cum : 0.f;
+      }
+    }
+  // ---- lights per band over slots, main.py:590-627 (float32 sums, CDF left unclamped)
+  std::vector<std::vector<int>> lights(B);
+  for (int s = 0; s < T; ++s)
+    for (int b = 0; b < B; ++b)
+      if (sd->mat_i32[(size_t)slot_mat[s] * 2 * B + 1 * B + b]) lights[b].push_back(s);
+  int L = 1;
+  for (int b = 0; b < B; ++b) L = std::max<int>(L, (int)lights[b].size());
+  std::vector<float> lcdf((size_t)B * L, 0.f), larea(B, 0.f);
+  std::vector<int32_t> lslot((size_t)B * L, 0), nl(B, 0);
+  for (int b = 0; b < B; ++b) {
+    nl[b] = (int)lights[b].size();
+    if (!nl[b]) continue;
+    float tot = 0.f;
+    for (int s : lights[b]) tot += sd->area[bvh.perm[s]];
+    larea[b] = tot;
+    float cum = 0.f;
+    for (int i = 0; i < nl[b]; ++i) {
+      cum += sd->area[bvh.perm[lights[b][i]]] / tot;
+      lcdf[(size_t)b * L + i] = cum;
+      lslot[(size_t)b * L + i] = lights[b][i];
+    }
+  }
+
+  // ---- upload (replace any previous scene)
+  free_list(c->scene_allocs);
+  c->has_scene = false;
+  c->scene_bytes = 0;
+  ts::DevScene ds{};
+  size_t &by = c->scene_bytes;
+  std::vector<void *> &ow = c->scene_allocs;
+  float4 *d_node, *d_tri, *d_shade, *d_mat;
+  float *d_rmin, *d_rmax, *d_eem, *d_qy, *d_cdf, *d_lcdf, *d_larea, *d_cmf;
+  int4 *d_rlink;
+  int32_t *d_meem, *d_lslot, *d_nl;
+  TS_CUDA(c, upload(c, ow, bvh.node2.data(), bvh.node2.size(), &d_node, by), "upload nodes");
+  TS_CUDA(c, upload(c, ow, tri.data(), tri.size(), &d_tri, by), "upload triangles");
+  TS_CUDA(c, upload(c, ow, shade.data(), shade.size(), &d_shade, by), "upload normals");
+  TS_CUDA(c, upload(c, ow, bvh.ref_min.data(), bvh.ref_min.size(), &d_rmin, by), "upload ref nodes");
+  TS_CUDA(c, upload(c, ow, bvh.ref_max.data(), bvh.ref_max.size(), &d_rmax, by), "upload ref nodes");
+  TS_CUDA(c, upload(c, ow, bvh.ref_link.data(), bvh.ref_link.size(), &d_rlink, by), "upload ref nodes");
+  TS_CUDA(c, upload(c, ow, mat.data(), mat.size(), &d_mat, by), "upload materials");
+  TS_CUDA(c, upload(c, ow, sd->mat_eem, (size_t)M, &d_meem, by), "upload materials");
+  TS_CUDA(c, upload(c, ow, eem.data(), eem.size(), &d_eem, by), "upload EEM");
+  TS_CUDA(c, upload(c, ow, qy.data(), qy.size(), &d_qy, by), "upload EEM");
+  TS_CUDA(c, upload(c, ow, cdf.data(), cdf.size(), &d_cdf, by), "upload EEM");
+  TS_CUDA(c, upload(c, ow, lcdf.data(), lcdf.size(), &d_lcdf, by), "upload lights");
+  TS_CUDA(c, upload(c, ow, lslot.data(), lslot.size(), &d_lslot, by), "upload lights");
+  TS_CUDA(c, upload(c, ow, nl.data(), nl.size(), &d_nl, by), "upload lights");
+  TS_CUDA(c, upload(c, ow, larea.data(), larea.size(), &d_larea, by), "upload lights");
+  TS_CUDA(c, upload(c, ow, sd->cmf, (size_t)3 * B, &d_cmf, by), "upload CMF");
+  ds.node = d_node;
+  ds.tri = d_tri;
+  ds.shade = d_shade;
+  ds.num_nodes = (int)(bvh.node2.size() / 4);
+  ds.num_tris = T;
+  ds.ref_min = d_rmin;
+  ds.ref_max = d_rmax;
+  ds.ref_link = d_rlink;
+  ds.num_ref_nodes = (int)bvh.ref_link.size();
+  ds.mat = d_mat;
+  ds.mat_eem = d_meem;
+  ds.eem = d_eem;
+  ds.eem_qy = d_qy;
+  ds.eem_cdf = d_cdf;
+  ds.num_materials = M;
+  ds.num_eems = E;
+  ds.light_cdf = d_lcdf;
+  ds.light_slot = d_lslot;
+  ds.num_lights = d_nl;
+  ds.light_area = d_larea;
+  ds.max_lights = L;
+  c->ds = ds;
+  c->d_cmf = d_cmf;
+  c->perm = bvh.perm;
+  c->info.num_tris = T;
+  c->info.num_nodes = ds.num_nodes;
+  c->info.num_ref_nodes = ds.num_ref_nodes;
+  c->info.max_depth = bvh.max_depth;
+  c->info.leaves = bvh.leaves;
+  c->info.sah_cost = bvh.sah_cost;
+  c->info.max_lights = L;
+  c->has_scene = true;
+  // keep the current camera basis
+  return ts_set_camera(c, c->cam, c->cam + 3, c->cam + 6);
+}
+
+ts_status ts_scene_info_get(const ts_ctx *c, ts_scene_info *info) {
+  if (!c || !info) return fail(nullptr, TS_ERR_INVALID_ARG, "ts_scene_info_get: null argument");
+  *info = c->info;
+  info->device_bytes = c->scene_bytes + c->film_bytes + c->wave_bytes;
+  return TS_OK;
+}
+
+ts_status ts_get_tri_perm(const ts_ctx *c, int32_t *perm_out) {
+  if (!c || !perm_out) return fail(nullptr, TS_ERR_INVALID_ARG, "ts_get_tri_perm: null argument");
+  std::copy(c->perm.begin(), c->perm.end(), perm_out);
+  return TS_OK;
+}
+
+ts_status ts_build_bvh_host(int32_t T, const float *v0, const float *v1, const float *v2, int32_t bins,
+                            int32_t leaf_max, float cost_trav, float cost_tri, int32_t max_nodes, float *nmin,
+                            float *nmax, int32_t *left, int32_t *right, int32_t *ntris, int32_t *tstart,
+                            int32_t *perm, int32_t *num_nodes_out) {
+  if (T < 0 || (T > 0 && (!v0 || !v1 || !v2 || !perm)) || !num_nodes_out)
+    return fail(nullptr, TS_ERR_INVALID_ARG, "ts_build_bvh_host: bad argument");
+  ts::BvhParams p;
+  if (bins > 0) p.bins = bins;
+  if (leaf_max > 0) p.leaf_max = std::min(leaf_max, ts::kLeafMax);
+  if (cost_trav > 0) p.cost_trav = cost_trav;
+  if (cost_tri > 0) p.cost_tri = cost_tri;
+  ts::BvhOut b;
+  std::string err;
+  if (!ts::build_bvh_binned(T, v0, v1, v2, p, b, err)) return fail(nullptr, TS_ERR_INVALID_ARG, "ts_build_bvh_host: " + err);
+  const int N = (int)b.ref_link.size();
+  *num_nodes_out = N;
+  if (N > max_nodes || (N > 0 && (!nmin || !nmax || !left || !right || !ntris || !tstart)))
+    return fail(nullptr, TS_ERR_CAPACITY, "ts_build_bvh_host: output arrays hold " + std::to_string(max_nodes) +
+                                              " nodes, " + std::to_string(N) + " needed");
+  std::copy(b.ref_min.begin(), b.ref_min.end(), nmin);
+  std::copy(b.ref_max.begin(), b.ref_max.end(), nmax);
+  for (int i = 0; i < N; ++i) {
+    left[i] = b.ref_link[i].x;
+    right[i] = b.ref_link[i].y;
+    ntris[i] = b.ref_link[i].z;
+    tstart[i] = b.ref_link[i].w;
+  }
+  std::copy(b.perm.begin(), b.perm.end(), perm);
+  return TS_OK;
+}
+
+ts_status ts_set_camera(ts_ctx *c, const float o[3], const float l[3], const float up[3]) {
+  if (!c || !o || !l || !up) return fail(c, TS_ERR_INVALID_ARG, "ts_set_camera: null argument");
+  float tmp[9] = {o[0], o[1], o[2], l[0], l[1], l[2], up[0], up[1], up[2]};
+  std::memcpy(c->cam, tmp, sizeof(tmp));
+  float3 w, u, v;
+  camera_basis(o, l, up, w, u, v);
+  c->ds.cam_o = make_float3(o[0], o[1], o[2]);
+  c->ds.cam_u = u;
+  c->ds.cam_v = v;
+  c->ds.cam_w = w;
+  return TS_OK;
+}
+
+static ts_status ensure_wave(ts_ctx *c);
+
+ts_status ts_render_pass(ts_ctx *c, uint32_t pass_idx, int32_t band, void *stream) {
+  if (!c) return fail(nullptr, TS_ERR_INVALID_ARG, "ts_render_pass: null context");
+  if (!c->has_scene) return fail(c, TS_ERR_NO_SCENE, "ts_render_pass: no scene uploaded");
+  if (band < 0 || band >= c->cfg.bands) return fail(c, TS_ERR_INVALID_ARG, "ts_render_pass: band out of range");
+  cudaSetDevice(c->cfg.device);
+  const cudaStream_t st = as_stream(stream);
+  const int bs = c->cfg.block_size;
+  if (c->cfg.kernel == TS_KERNEL_MEGA) {
+    int per_sm = c->cfg.blocks_per_sm;
+    if (per_sm <= 0) per_sm = std::max(1, 2048 / bs);
+    const int grid = c->num_sms * per_sm;
+    TS_CUDA(c, ts::launch_render_mega(c->ds, c->dc, pass_idx, band, film_of(c), c->d_counter, c->d_err, grid, bs, st),
+            "render pass");
+  } else {
+    ts_status s = ensure_wave(c);
+    if (s != TS_OK) return s;
+    int per_sm = c->cfg.blocks_per_sm;
+    if (per_sm <= 0) per_sm = std::max(1, 2048 / bs);
+    const int grid = c->num_sms * per_sm;
+    TS_CUDA(c, ts::launch_wave_pass(c->ds, c->dc, pass_idx, band, film_of(c), c->wave, c->d_err, grid, bs,
+                                    c->cfg.sort_keys, st),
+            "render pass");
+  }
+  return TS_OK;
+}
+
+ts_status ts_accumulate_block(ts_ctx *c, int32_t n, void *stream) {
+  if (!c) return fail(nullptr, TS_ERR_INVALID_ARG, "ts_accumulate_block: null context");
+  if (n < 1) return fail(c, TS_ERR_INVALID_ARG, "ts_accumulate_block: num_blocks_completed must be >= 1");
+  cudaSetDevice(c->cfg.device);
+  TS_CUDA(c, ts::launch_accumulate_block(film_of(c), n, as_stream(stream)), "accumulate");
+  return TS_OK;
+}
+
+ts_status ts_reset(ts_ctx *c, void *stream) {
+  if (!c) return fail(nullptr, TS_ERR_INVALID_ARG, "ts_reset: null context");
+  cudaSetDevice(c->cfg.device);
+  TS_CUDA(c, ts::launch_clear_film(film_of(c), as_stream(stream)), "reset");
+  return TS_OK;
+}
+
+ts_status ts_film_buffer(ts_ctx *c, int32_t which, double **dev_ptr, size_t *count) {
+  if (!c || !dev_ptr || !count || which < 0 || which > 2)
+    return fail(c, TS_ERR_INVALID_ARG, "ts_film_buffer: bad argument");
+  *dev_ptr = c->d_film[which];
+  *count = (size_t)c->cfg.width * c->cfg.height * c->cfg.bands;
+  return TS_OK;
+}
+
+ts_status ts_film_download(ts_ctx *c, int32_t which, double *host, void *stream) {
+  if (!c || !host || which < 0 || which > 2) return fail(c, TS_ERR_INVALID_ARG, "ts_film_download: bad argument");
+  cudaSetDevice(c->cfg.device);
+  const size_t n = (size_t)c->cfg.width * c->cfg.height * c->cfg.bands;
+  TS_CUDA(c, cudaMemcpyAsync(host, c->d_film[which], n * sizeof(double), cudaMemcpyDeviceToHost, as_stream(stream)),
+          "film download");
+  TS_CUDA(c, cudaStreamSynchronize(as_stream(stream)), "film download");
+  return TS_OK;
+}
+
+ts_status ts_resolve_xyz(ts_ctx *c, double scale, float *xyz_dev, void *stream) {
+  if (!c || !xyz_dev) return fail(c, TS_ERR_INVALID_ARG, "ts_resolve_xyz: bad argument");
+  if (!c->has_scene) return fail(c, TS_ERR_NO_SCENE, "ts_resolve_xyz: no scene (CMF) uploaded");
+  cudaSetDevice(c->cfg.device);
+  TS_CUDA(c, ts::launch_resolve_xyz(film_of(c), c->d_cmf, scale, xyz_dev, as_stream(stream)), "resolve xyz");
+  return TS_OK;
+}
+
+ts_status ts_resolve_xyz_host(ts_ctx *c, double scale, float *xyz_host, void *stream) {
+  if (!c || !xyz_host) return fail(c, TS_ERR_INVALID_ARG, "ts_resolve_xyz_host: bad argument");
+  ts_status s = ts_resolve_xyz(c, scale, c->d_xyz, stream);
+  if (s != TS_OK) return s;
+  const size_t n = (size_t)c->cfg.width * c->cfg.height * 3;
+  TS_CUDA(c, cudaMemcpyAsync(xyz_host, c->d_xyz, n * sizeof(float), cudaMemcpyDeviceToHost, as_stream(stream)),
+          "resolve xyz copy");
+  TS_CUDA(c, cudaStreamSynchronize(as_stream(stream)), "resolve xyz sync");
+  return TS_OK;
+}
+
+ts_status ts_resolve_rgb(ts_ctx *c, double scale, const float M[9], float exposure, float gamma, int32_t iw,
+                         int32_t ih, float *rgb_dev, void *stream) {
+  if (!c || !M || !rgb_dev || iw <= 0 || ih <= 0) return fail(c, TS_ERR_INVALID_ARG, "ts_resolve_rgb: bad argument");
+  if (!c->has_scene) return fail(c, TS_ERR_NO_SCENE, "ts_resolve_rgb: no scene (CMF) uploaded");
+  cudaSetDevice(c->cfg.device);
+  TS_CUDA(c, cudaMemcpyAsync(c->d_m9, M, 9 * sizeof(float), cudaMemcpyHostToDevice, as_stream(stream)),
+          "resolve rgb matrix");
+  TS_CUDA(c, ts::launch_resolve_rgb(film_of(c), c->d_cmf, scale, c->d_m9, exposure, gamma, iw, ih, rgb_dev,
+                                    as_stream(stream)),
+          "resolve rgb");
+  return TS_OK;
+}
+
+ts_status ts_trace_batch(ts_ctx *c, const float *rays, int32_t n, int32_t mode, int32_t *tri, float *t, float *u,
+                         float *v, void *stream) {
+  if (!c || n < 0 || (n > 0 && (!rays || !tri || !t))) return fail(c, TS_ERR_INVALID_ARG, "ts_trace_batch: bad argument");
+  if (mode != TS_TRACE_FAST && mode != TS_TRACE_REFERENCE_ORDER)
+    return fail(c, TS_ERR_INVALID_ARG, "ts_trace_batch: unknown mode");
+  if (!c->has_scene) return fail(c, TS_ERR_NO_SCENE, "ts_trace_batch: no scene uploaded");
+  cudaSetDevice(c->cfg.device);
+  TS_CUDA(c, ts::launch_trace_batch(c->ds, c->dc.eps, rays, n, mode, tri, t, u, v, c->d_err, as_stream(stream)),
+          "trace batch");
+  return TS_OK;
+}
+
+ts_status ts_render_normals(ts_ctx *c, float *out, void *stream) {
+  if (!c || !out) return fail(c, TS_ERR_INVALID_ARG, "ts_render_normals: bad argument");
+  if (!c->has_scene) return fail(c, TS_ERR_NO_SCENE, "ts_render_normals: no scene uploaded");
+  cudaSetDevice(c->cfg.device);
+  TS_CUDA(c, ts::launch_render_normals(c->ds, c->dc, out, c->d_err, as_stream(stream)), "render normals");
+  return TS_OK;
+}
+
+ts_status ts_check_device(ts_ctx *c, uint32_t *bits) {
+  if (!c || !bits) return fail(c, TS_ERR_INVALID_ARG, "ts_check_device: bad argument");
+  cudaSetDevice(c->cfg.device);
+  TS_CUDA(c, cudaDeviceSynchronize(), "device synchronise");
+  TS_CUDA(c, cudaMemcpy(bits, c->d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost), "read device status");
+  TS_CUDA(c, cudaMemset(c->d_err, 0, sizeof(uint32_t)), "clear device status");
+  if (*bits) {
+    std::string m = "device reported:";
+    if (*bits & ts::kErrStackOverflow) m += " traversal stack overflow;";
+    if (*bits & ts::kErrQueueOverflow) m += " queue overflow;";
+    if (*bits & ts::kErrIterationCap) m += " iteration cap reached;";
+    return fail(c, TS_ERR_DEVICE_FAULT, m);
+  }
+  return TS_OK;
+}
+
+}  // extern "C"
+
+// wavefront buffers are created on first use (one slot per pixel)
+static ts_status ensure_wave(ts_ctx *c) {
+  const int n = c->cfg.width * c->cfg.height;
+  if (c->wave.capacity >= n) return TS_OK;
+  free_list(c->wave_allocs);
+  c->wave = ts::WaveBuffers{};
+  c->wave_bytes = 0;
+  auto grab = [&](void **p, size_t bytes) -> cudaError_t {
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e == cudaSuccess) {
+      c->wave_allocs.push_back(*p);
+      c->wave_bytes += bytes;
+    }
+    return e;
+  };
+  ts::WaveBuffers &w = c->wave;
+  const size_t N = (size_t)n;
+  TS_CUDA(c, grab((void **)&w.pos_thr, N * sizeof(float4)), "wavefront buffers");
+  TS_CUDA(c, grab((void **)&w.dir_spdf, N * sizeof(float4)), "wavefront buffers");
+  TS_CUDA(c, grab((void **)&w.meta, N * sizeof(int4)), "wavefront buffers");
+  TS_CUDA(c, grab((void **)&w.hit, N * sizeof(float4)), "wavefront buffers");
+  TS_CUDA(c, grab((void **)&w.sq_origin, N * sizeof(float4)), "wavefront buffers");
+  TS_CUDA(c, grab((void **)&w.sq_dir, N * sizeof(float4)), "wavefront buffers");
+  TS_CUDA(c, grab((void **)&w.sq_meta, N * sizeof(int4)), "wavefront buffers");
+  TS_CUDA(c, grab((void **)&w.queue[0], N * sizeof(int)), "wavefront buffers");
+  TS_CUDA(c, grab((void **)&w.queue[1], N * sizeof(int)), "wavefront buffers");
+  TS_CUDA(c, grab((void **)&w.shadow_queue, N * sizeof(int)), "wavefront buffers");
+  TS_CUDA(c, grab((void **)&w.sorted, N * sizeof(int)), "wavefront buffers");
+  TS_CUDA(c, grab((void **)&w.counts, 8192 * sizeof(int)), "wavefront buffers");
+  TS_CUDA(c, grab((void **)&w.key_hist, 2 * ts::kMaxKeys * sizeof(int)), "wavefront buffers");
+  w.capacity = n;
+  return TS_OK;
+}

@@ -1,0 +1,422 @@
+// Host BVH builder (binned SAH, multi-threaded over large subtrees) and
+// converters to the device layouts.
+//
+// The reference builds its tree with a full sweep over every split position
+// (build_bvh, main.py:437-507), which is quadratic per node and takes minutes
+// beyond ~10k triangles.  Binning the centroids (Wald, "On fast construction
+// of SAH-based bounding volume hierarchies", 2007) gives trees of comparable
+// quality in O(n log n); closest-hit results do not depend on the tree.
+#include "bvh.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <future>
+#include <thread>
+
+#include "limits.h"
+
+namespace ts {
+
+namespace {
+
+struct Prim {
+  float lo[3], hi[3], c[3];
+};
+
+struct BNode {
+  float lo[3], hi[3];
+  int32_t left, right;  // child indices within the same vector; -1 for leaves
+  int32_t first, count;
+};
+
+// Flat boxes make the strict t_enter < t_exit slab test fail for rays that hit
+// the face they lie in, so a zero extent is widened (the reference adds 1e-6,
+// main.py:456-460; here at least a few ulps of the coordinate as well).
+inline void pad_box(float lo[3], float hi[3]) {
+  for (int a = 0; a < 3; ++a) {
+    if (lo[a] == hi[a]) {
+      const float p = std::max(1e-6f, std::fabs(lo[a]) * 4.8e-7f);
+      lo[a] -= p;
+      hi[a] += p;
+    }
+  }
+}
+
+inline double half_area(const float lo[3], const float hi[3]) {
+  const double dx = std::max(0.0, (double)hi[0] - lo[0]);
+  const double dy = std::max(0.0, (double)hi[1] - lo[1]);
+  const double dz = std::max(0.0, (double)hi[2] - lo[2]);
+  return dx * dy + dy * dz + dz * dx;
+}
+
+struct Builder {
+  const std::vector<Prim> &prims;
+  std::vector<int32_t> &idx;
+  BvhParams p;
+
+  void bounds(int b, int e, float lo[3], float hi[3], float clo[3], float chi[3]) const {
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = clo[a] = INFINITY;
+      hi[a] = chi[a] = -INFINITY;
+    }
+    for (int i = b; i < e; ++i) {
+      const Prim &q = prims[idx[i]];
+      for (int a = 0; a < 3; ++a) {
+        lo[a] = std::min(lo[a], q.lo[a]);
+        hi[a] = std::max(hi[a], q.hi[a]);
+        clo[a] = std::min(clo[a], q.c[a]);
+        chi[a] = std::max(chi[a], q.c[a]);
+      }
+    }
+  }
+
+  int median_split(int b, int e, const float clo[3], const float chi[3]) {
+    int ax = 0;
+    for (int a = 1; a < 3; ++a)
+      if (chi[a] - clo[a] > chi[ax] - clo[ax]) ax = a;
+    const int mid = b + (e - b) / 2;
+    std::nth_element(idx.begin() + b, idx.begin() + mid, idx.begin() + e,
+                     [&](int32_t x, int32_t y) { return prims[x].c[ax] < prims[y].c[ax]; });
+    return mid;
+  }
+
+  // Fills node's box; returns the split position or -1 for a leaf.
+  int decide(int b, int e, int depth, BNode &node) {
+    float clo[3], chi[3];
+    bounds(b, e, node.lo, node.hi, clo, chi);
+    pad_box(node.lo, node.hi);
+    const int n = e - b;
+    node.left = node.right = -1;
+    node.first = b;
+    node.count = n;
+    if (n <= 1) return -1;
+    const int hard_max = std::min(p.leaf_max, kLeafMax);
+    if (depth >= p.sah_depth) return n <= hard_max ? -1 : median_split(b, e, clo, chi);
+    const int K = std::max(2, std::min(p.bins, 256));
+    double best = INFINITY;
+    int best_axis = -1, best_bin = -1;
+    std::vector<float> blo(3 * K), bhi(3 * K), rlo(3 * K), rhi(3 * K);
+    std::vector<int> bc(K);
+    std::vector<double> racc(K);
+    std::vector<int> rcnt(K);
+    for (int a = 0; a < 3; ++a) {
+      const float ext = chi[a] - clo[a];
+      if (!(ext > 0.f)) continue;
+      const float k = (float)K * (1.0f - 1e-6f) / ext;
+      std::fill(bc.begin(), bc.end(), 0);
+      for (int i = 0; i < K; ++i)
+        for (int d = 0; d < 3; ++d) {
+          blo[3 * i + d] = INFINITY;
+          bhi[3 * i + d] = -INFINITY;
+        }
+      for (int i = b; i < e; ++i) {
+        const Prim &q = prims[idx[i]];
+        int bi = (int)((q.c[a] - clo[a]) * k);
+        bi = std::min(std::max(bi, 0), K - 1);
+        bc[bi]++;
+        for (int d = 0; d < 3; ++d) {
+          blo[3 * bi + d] = std::min(blo[3 * bi + d], q.lo[d]);
+          bhi[3 * bi + d] = std::max(bhi[3 * bi + d], q.hi[d]);
+        }
+      }
+      // right-to-left accumulation
+      float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+      int cnt = 0;
+      for (int i = K - 1; i > 0; --i) {
+        for (int d = 0; d < 3; ++d) {
+          lo[d] = std::min(lo[d], blo[3 * i + d]);
+          hi[d] = std::max(hi[d], bhi[3 * i + d]);
+        }
+        cnt += bc[i];
+        rcnt[i] = cnt;
+        racc[i] = cnt ? half_area(lo, hi) * cnt : 0.0;
+      }
+      for (int d = 0; d < 3; ++d) { lo[d] = INFINITY; hi[d] = -INFINITY; }
+      cnt = 0;
+      for (int i = 0; i < K - 1; ++i) {
+        for (int d = 0; d < 3; ++d) {
+          lo[d] = std::min(lo[d], blo[3 * i + d]);
+          hi[d] = std::max(hi[d], bhi[3 * i + d]);
+        }
+        cnt += bc[i];
+        if (cnt == 0 || rcnt[i + 1] == 0) continue;
+        const double c = half_area(lo, hi) * cnt + racc[i + 1];
+        if (c < best) { best = c; best_axis = a; best_bin = i; }
+      }
+    }
+    if (best_axis < 0) return n <= kLeafMax ? -1 : median_split(b, e, clo, chi);
+    const double A = half_area(node.lo, node.hi);
+    const double split_cost = p.cost_trav + p.cost_tri * (A > 0 ? best / A : (double)n);
+    const double leaf_cost = p.cost_tri * n;
+    if (n <= hard_max && leaf_cost <= split_cost) return -1;
+    const float ext = chi[best_axis] - clo[best_axis];
+    const float k = (float)K * (1.0f - 1e-6f) / ext;
+    auto it = std::partition(idx.begin() + b, idx.begin() + e, [&](int32_t t) {
+      int bi = (int)((prims[t].c[best_axis] - clo[best_axis]) * k);
+      bi = std::min(std::max(bi, 0), K - 1);
+      return bi <= best_bin;
+    });
+    int mid = (int)(it - idx.begin());
+    if (mid == b || mid == e) mid = median_split(b, e, clo, chi);
+    return mid;
+  }
+
+  int rec(std::vector<BNode> &out, int b, int e, int depth) {
+    const int me = (int)out.size();
+    out.push_back(BNode{});
+    BNode node;
+    const int mid = decide(b, e, depth, node);
+    out[me] = node;
+    if (mid < 0) return me;
+    const int l = rec(out, b, mid, depth + 1);
+    const int r = rec(out, mid, e, depth + 1);
+    out[me].left = l;
+    out[me].right = r;
+    return me;
+  }
+
+  std::vector<BNode> task(int b, int e, int depth, int par_levels) {
+    std::vector<BNode> out;
+    if (par_levels <= 0 || e - b < 65536) {
+      out.reserve((size_t)(2 * (e - b) / 3 + 16));
+      rec(out, b, e, depth);
+      return out;
+    }
+    BNode root;
+    const int mid = decide(b, e, depth, root);
+    if (mid < 0) {
+      out.push_back(root);
+      return out;
+    }
+    auto fl = std::async(std::launch::async, [&, b, mid]() { return task(b, mid, depth + 1, par_levels - 1); });
+    std::vector<BNode> r = task(mid, e, depth + 1, par_levels - 1);
+    std::vector<BNode> l = fl.get();
+    out.reserve(1 + l.size() + r.size());
+    out.push_back(root);
+    auto append = [&](const std::vector<BNode> &v, int off) {
+      for (BNode x : v) {
+        if (x.left >= 0) { x.left += off; x.right += off; }
+        out.push_back(x);
+      }
+    };
+    out[0].left = 1;
+    out[0].right = 1 + (int)l.size();
+    append(l, 1);
+    append(r, 1 + (int)l.size());
+    return out;
+  }
+};
+
+inline int32_t leaf_code(int first, int count) { return ~((first << 4) | (count - 1)); }
+
+// Flatten a preorder BNode tree into the two-child layout.  Leaves larger than
+// kLeafMax are split into index chunks.  Returns false on a malformed tree.
+bool flatten_two_child(std::vector<BNode> tree, const std::vector<Prim> &prims, const std::vector<int32_t> &perm,
+                       BvhOut &out, std::string &err) {
+  // expand oversized leaves
+  for (size_t i = 0; i < tree.size(); ++i) {
+    BNode nd = tree[i];
+    if (nd.left < 0 && nd.count > kLeafMax) {
+      const int half = nd.count / 2;
+      BNode a{}, c{};
+      for (int s = 0; s < 2; ++s) {
+        BNode &ch = s ? c : a;
+        ch.first = s ? nd.first + half : nd.first;
+        ch.count = s ? nd.count - half : half;
+        ch.left = ch.right = -1;
+        for (int d = 0; d < 3; ++d) { ch.lo[d] = INFINITY; ch.hi[d] = -INFINITY; }
+        for (int k = ch.first; k < ch.first + ch.count; ++k)
+          for (int d = 0; d < 3; ++d) {
+            ch.lo[d] = std::min(ch.lo[d], prims[perm[k]].lo[d]);
+            ch.hi[d] = std::max(ch.hi[d], prims[perm[k]].hi[d]);
+          }
+        pad_box(ch.lo, ch.hi);
+      }
+      tree[i].left = (int)tree.size();
+      tree.push_back(a);
+      tree[i].right = (int)tree.size();
+      tree.push_back(c);
+    }
+  }
+  const int N = (int)tree.size();
+  if (N == 0) {
+    out.node2.clear();
+    return true;
+  }
+  // number the inner nodes (depth-first, children in left/right order)
+  std::vector<int> map(N, -1), depth(N, 0);
+  std::vector<int> stack = {0};
+  int inner = 0, leaves = 0, maxd = 0;
+  std::vector<char> seen(N, 0);
+  while (!stack.empty()) {
+    const int i = stack.back();
+    stack.pop_back();
+    if (i < 0 || i >= N || seen[i]) {
+      err = "BVH: malformed tree (bad or repeated child index)";
+      return false;
+    }
+    seen[i] = 1;
+    maxd = std::max(maxd, depth[i]);
+    if (tree[i].left >= 0) {
+      map[i] = inner++;
+      const int l = tree[i].left, r = tree[i].right;
+      if (l < 0 || l >= N || r < 0 || r >= N) {
+        err = "BVH: child index out of range";
+        return false;
+      }
+      depth[l] = depth[r] = depth[i] + 1;
+      stack.push_back(r);
+      stack.push_back(l);
+    } else {
+      ++leaves;
+    }
+  }
+  if (maxd + 1 >= kStackDepth) {
+    err = "BVH: tree depth " + std::to_string(maxd) + " exceeds the traversal stack";
+    return false;
+  }
+  const bool root_leaf = tree[0].left < 0;
+  const int nodes = root_leaf ? 1 : inner;
+  out.node2.assign((size_t)4 * nodes, make_float4(0.f, 0.f, 0.f, 0.f));
+  auto child_ref = [&](int c) { return tree[c].left >= 0 ? map[c] : leaf_code(tree[c].first, tree[c].count); };
+  auto put = [&](int slot, int c0, int c1, bool c1_empty) {
+    const BNode &A = tree[c0];
+    const float nanf_ = std::nanf("");
+    float b1[6];
+    if (c1_empty) {
+      for (float &x : b1) x = nanf_;
+    } else {
+      const BNode &Bn = tree[c1];
+      b1[0] = Bn.lo[0]; b1[1] = Bn.hi[0]; b1[2] = Bn.lo[1]; b1[3] = Bn.hi[1]; b1[4] = Bn.lo[2]; b1[5] = Bn.hi[2];
+    }
+    out.node2[4 * slot + 0] = make_float4(A.lo[0], A.hi[0], A.lo[1], A.hi[1]);
+    out.node2[4 * slot + 1] = make_float4(b1[0], b1[1], b1[2], b1[3]);
+    out.node2[4 * slot + 2] = make_float4(A.lo[2], A.hi[2], b1[4], b1[5]);
+    int4 link = make_int4(child_ref(c0), c1_empty ? child_ref(c0) : child_ref(c1), 0, 0);
+    std::memcpy(&out.node2[4 * slot + 3], &link, sizeof(int4));
+  };
+  if (root_leaf) {
+    put(0, 0, 0, true);
+  } else {
+    for (int i = 0; i < N; ++i)
+      if (tree[i].left >= 0) put(map[i], tree[i].left, tree[i].right, false);
+  }
+  out.max_depth = maxd;
+  out.leaves = leaves;
+  return true;
+}
+
+std::vector<Prim> make_prims(int T, const float *v0, const float *v1, const float *v2) {
+  std::vector<Prim> prims(T);
+  for (int t = 0; t < T; ++t) {
+    Prim &q = prims[t];
+    for (int a = 0; a < 3; ++a) {
+      const float x = v0[3 * t + a], y = v1[3 * t + a], z = v2[3 * t + a];
+      q.lo[a] = std::min(std::min(x, y), z);
+      q.hi[a] = std::max(std::max(x, y), z);
+      q.c[a] = ((x + y) + z) / 3.0f;
+    }
+  }
+  return prims;
+}
+
+}  // namespace
+
+bool build_bvh_binned(int T, const float *v0, const float *v1, const float *v2, const BvhParams &p, BvhOut &out,
+                      std::string &err) {
+  out = BvhOut{};
+  if (T < 0 || T >= (1 << 27)) {
+    err = "BVH: triangle count out of range (0 .. 2^27-1)";
+    return false;
+  }
+  out.perm.resize(T);
+  for (int i = 0; i < T; ++i) out.perm[i] = i;
+  if (T == 0) return true;
+  std::vector<Prim> prims = make_prims(T, v0, v1, v2);
+  Builder b{prims, out.perm, p};
+  unsigned hw = p.threads > 0 ? (unsigned)p.threads : std::max(1u, std::thread::hardware_concurrency());
+  int par_levels = 0;
+  while ((1u << par_levels) < hw && par_levels < 6) ++par_levels;
+  std::vector<BNode> tree = b.task(0, T, 0, par_levels);
+  // reference layout: same preorder numbering
+  const int N = (int)tree.size();
+  out.ref_min.resize(3 * (size_t)N);
+  out.ref_max.resize(3 * (size_t)N);
+  out.ref_link.resize(N);
+  double cost = 0.0;
+  const double root_area = half_area(tree[0].lo, tree[0].hi);
+  for (int i = 0; i < N; ++i) {
+    const BNode &nd = tree[i];
+    for (int a = 0; a < 3; ++a) {
+      out.ref_min[3 * i + a] = nd.lo[a];
+      out.ref_max[3 * i + a] = nd.hi[a];
+    }
+    const double a = root_area > 0 ? half_area(nd.lo, nd.hi) / root_area : 1.0;
+    if (nd.left >= 0) {
+      out.ref_link[i] = make_int4(nd.left, nd.right, 0, 0);
+      cost += p.cost_trav * a;
+    } else {
+      out.ref_link[i] = make_int4(-1, -1, nd.count, nd.first);
+      cost += p.cost_tri * a * nd.count;
+    }
+  }
+  out.sah_cost = cost;
+  return flatten_two_child(std::move(tree), prims, out.perm, out, err);
+}
+
+bool bvh_from_reference(int T, const float *v0, const float *v1, const float *v2, int N, const float *nmin,
+                        const float *nmax, const int32_t *left, const int32_t *right, const int32_t *ntris,
+                        const int32_t *tstart, const int32_t *perm, BvhOut &out, std::string &err) {
+  out = BvhOut{};
+  if (T < 0 || T >= (1 << 27) || N < 0 || (T > 0 && N == 0)) {
+    err = "BVH: bad triangle or node count";
+    return false;
+  }
+  out.perm.assign(perm, perm + T);
+  {
+    std::vector<char> used(T, 0);
+    for (int i = 0; i < T; ++i) {
+      if (perm[i] < 0 || perm[i] >= T || used[perm[i]]) {
+        err = "BVH: permutation is not a permutation of the triangles";
+        return false;
+      }
+      used[perm[i]] = 1;
+    }
+  }
+  if (T == 0) return true;
+  std::vector<Prim> prims = make_prims(T, v0, v1, v2);
+  std::vector<BNode> tree(N);
+  out.ref_min.assign(nmin, nmin + 3 * (size_t)N);
+  out.ref_max.assign(nmax, nmax + 3 * (size_t)N);
+  out.ref_link.resize(N);
+  for (int i = 0; i < N; ++i) {
+    BNode &b = tree[i];
+    for (int a = 0; a < 3; ++a) {
+      b.lo[a] = nmin[3 * i + a];
+      b.hi[a] = nmax[3 * i + a];
+    }
+    if (ntris[i] > 0) {
+      if (tstart[i] < 0 || tstart[i] + ntris[i] > T) {
+        err = "BVH: leaf triangle range out of bounds";
+        return false;
+      }
+      b.left = b.right = -1;
+      b.first = tstart[i];
+      b.count = ntris[i];
+      out.ref_link[i] = make_int4(-1, -1, ntris[i], tstart[i]);
+    } else {
+      if (left[i] < 0 || left[i] >= N || right[i] < 0 || right[i] >= N) {
+        err = "BVH: inner node child out of range";
+        return false;
+      }
+      b.left = left[i];
+      b.right = right[i];
+      b.first = b.count = 0;
+      out.ref_link[i] = make_int4(left[i], right[i], 0, 0);
+    }
+  }
+  return flatten_two_child(std::move(tree), prims, out.perm, out, err);
+}
+
+}  // namespace ts

@@ -1,0 +1,40 @@
+// Host-side BVH construction and conversion to the device layouts.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+namespace ts {
+
+struct BvhParams {
+  int bins = 32;          // SAH bins per axis
+  float cost_trav = 1.0f; // SAH traversal cost (relative to one triangle test)
+  float cost_tri = 1.0f;
+  int leaf_max = 8;       // largest leaf the SAH may choose (hard cap 16)
+  int sah_depth = 40;     // below this depth, object-median splits only (bounds the tree depth)
+  int threads = 0;        // 0 = hardware concurrency
+};
+
+struct BvhOut {
+  std::vector<int32_t> perm;   // slot -> original triangle index
+  std::vector<float4> node2;   // two-child layout, 4 x float4 per node
+  std::vector<float> ref_min, ref_max;  // reference layout, [N][3]
+  std::vector<int4> ref_link;           // (left, right, num_tris, tri_start)
+  int max_depth = 0;
+  int leaves = 0;
+  double sah_cost = 0.0;
+};
+
+// Binned-SAH build over the triangles' bounding boxes and centroids.
+bool build_bvh_binned(int T, const float *v0, const float *v1, const float *v2, const BvhParams &p, BvhOut &out,
+                      std::string &err);
+
+// Adopt a tree given in the reference layout (e.g. produced by the reference's
+// own build_bvh, main.py:437-507): perm[slot] = original triangle index.
+bool bvh_from_reference(int T, const float *v0, const float *v1, const float *v2, int N, const float *nmin,
+                        const float *nmax, const int32_t *left, const int32_t *right, const int32_t *ntris,
+                        const int32_t *tstart, const int32_t *perm, BvhOut &out, std::string &err);
+
+}  // namespace ts

@@ -1,0 +1,59 @@
+// Host-side launchers of the device kernels (implemented in *.cu files).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace ts {
+
+// Film layout: [band][row j][column i] FP64, band-major so that one warp of
+// neighbouring pixels depositing into the same band writes 256 contiguous bytes.
+struct Film {
+  double *block;  // current block's per-band sums (block_accumulator)
+  double *mean;   // running mean over completed blocks (spectral_accumulator)
+  double *m2;     // sum over blocks of block^2 (for the per-pixel standard error)
+  int W, H, B;
+};
+
+// one sample pass (cast_rays): persistent megakernel with per-lane path regeneration
+cudaError_t launch_render_mega(const DevScene &s, const DevConfig &c, uint32_t pass, int band, Film f,
+                               int *counter, uint32_t *err, int grid, int block, cudaStream_t st);
+
+// closest hit for a ray batch; mode 0 = fast traversal, 1 = reference order
+cudaError_t launch_trace_batch(const DevScene &s, float eps, const float *rays, int n, int mode, int32_t *tri_orig,
+                               float *t, float *u, float *v, uint32_t *err, cudaStream_t st);
+
+cudaError_t launch_accumulate_block(Film f, int num_blocks_completed, cudaStream_t st);
+cudaError_t launch_clear_film(Film f, cudaStream_t st);
+cudaError_t launch_resolve_xyz(Film f, const float *cmf, double scale, float *xyz, cudaStream_t st);
+cudaError_t launch_resolve_rgb(Film f, const float *cmf, double scale, const float *xyz_to_rgb, float exposure,
+                               float gamma, int img_w, int img_h, float *rgb, cudaStream_t st);
+cudaError_t launch_render_normals(const DevScene &s, const DevConfig &c, float *out, uint32_t *err,
+                                  cudaStream_t st);
+
+// ---- wavefront renderer -------------------------------------------------------
+struct WaveBuffers {
+  // path state, one slot per pixel
+  float4 *pos_thr;    // pos.xyz, throughput
+  float4 *dir_spdf;   // dir.xyz, surface pdf
+  int4 *meta;         // (pixel, active | active_px << 8 | plen << 16, vol, rng draw index)
+  float4 *hit;        // (t, u, v, slot bits) of the last extension trace
+  // shadow queries, one slot per queued path
+  float4 *sq_origin;  // origin.xyz, max_dist
+  float4 *sq_dir;     // dir.xyz, contrib
+  int4 *sq_meta;      // (pixel, light_slot, vol, band)
+  int *queue[2];      // extension queues (ping-pong), path ids
+  int *shadow_queue;  // shadow queue, query ids == path ids
+  int *sorted;        // extension queue ordered by material key
+  int *counts;        // [2*max_depth + 8]: ext counts per depth, shadow counts per depth, scratch
+  int *key_hist;      // material-key histogram / offsets [kMaxKeys * 2]
+  int capacity;
+};
+constexpr int kMaxKeys = 256;
+
+cudaError_t launch_wave_pass(const DevScene &s, const DevConfig &c, uint32_t pass, int band, Film f,
+                             const WaveBuffers &w, uint32_t *err, int grid, int block, int sort_keys,
+                             cudaStream_t st);
+
+}  // namespace ts

@@ -1,0 +1,7 @@
+// Structural limits shared by the host builder and the device traversal.
+#pragma once
+
+namespace ts {
+constexpr int kStackDepth = 64;  // traversal stack entries per ray (bounds the tree depth)
+constexpr int kLeafMax = 16;     // triangles per leaf in the two-child layout (4-bit count)
+}  // namespace ts

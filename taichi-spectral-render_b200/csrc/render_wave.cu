@@ -1,0 +1,277 @@
+// Wavefront renderer: one sample pass as a fixed sequence of stage kernels
+// joined by compacted queues in device memory.
+//
+//   generate            camera rays for every pixel -> extension queue Q0
+//   trace(k)            closest hit for every path in Qk, and the whole shadow
+//                       chain (<= scatter_bounces segments) of every query
+//                       left by shade(k-1); direct light is deposited here
+//   shade(k)            volume event, emitter hit, next-event setup and surface
+//                       scatter for every path of Qk -> Q(k+1), shadow queries
+//   trace(depth)        the last shadow queries
+//
+// Path state lives in SoA arrays indexed by pixel; queues hold pixel ids.
+// Every stage fetches work 32 items at a time with one atomic per warp, so
+// the grid is persistent (a multiple of the SM count) and independent of
+// queue lengths, which are only known on the device.  Each pixel owns one
+// path per pass and stages run in stream order, so film deposits need no
+// atomics.  With sort_keys set, the shading queue is reordered by the hit
+// material (a counting sort on the device) so that warps shade one material
+// at a time.
+#include "estimator.cuh"
+#include "kernels.cuh"
+
+namespace ts {
+
+namespace {
+
+// layout of WaveBuffers::counts
+constexpr int kMaxDepth = 1024;
+constexpr int kCntExt = 0;                      // [kMaxDepth+1] extension queue lengths
+constexpr int kCntSh = kCntExt + kMaxDepth + 1;  // [kMaxDepth+1] shadow queue lengths
+constexpr int kCntFetchT = kCntSh + kMaxDepth + 1;
+constexpr int kCntFetchS = kCntFetchT + kMaxDepth + 1;
+constexpr int kCntTotal = kCntFetchS + kMaxDepth + 1;
+
+__device__ __forceinline__ int warp_fetch(int *ctr) {
+  const int lane = threadIdx.x & 31;
+  int base = 0;
+  if (lane == 0) base = atomicAdd(ctr, 32);
+  return __shfl_sync(0xffffffffu, base, 0);
+}
+
+// append with one atomic per warp; returns the slot for lanes with want=true
+__device__ __forceinline__ int warp_append(int *ctr, bool want) {
+  const unsigned m = __ballot_sync(0xffffffffu, want);
+  if (!m) return -1;
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(m) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(ctr, __popc(m));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  return want ? base + __popc(m & ((1u << lane) - 1u)) : -1;
+}
+
+__device__ __forceinline__ void deposit(const Film &f, int pixel, int band, float v) {
+  if (v != 0.f) f.block[(size_t)band * f.W * f.H + pixel] += (double)v;
+}
+
+__global__ void k_generate(DevScene s, DevConfig c, uint32_t pass, int band, WaveBuffers w) {
+  const int npix = c.W * c.H;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
+    Rng rng;
+    rng.init(c.seed, pass, (uint32_t)p, c.scene_id);
+    PathState ps;
+    camera_ray(s, c, p % c.W, p / c.W, rng, ps, band);
+    w.pos_thr[p] = make_float4(ps.pos.x, ps.pos.y, ps.pos.z, ps.thr);
+    w.dir_spdf[p] = make_float4(ps.dir.x, ps.dir.y, ps.dir.z, ps.spdf);
+    w.meta[p] = make_int4(p, band | (band << 8), 0, (int)rng.n);
+    w.queue[0][p] = p;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) w.counts[kCntExt + 0] = npix;
+}
+
+// trace(k): shadow chains of shade(k-1), then extension hits of Qk
+__global__ void __launch_bounds__(128) k_trace(DevScene s, DevConfig c, int depth, Film f, WaveBuffers w,
+                                               uint32_t *__restrict__ err) {
+  uint32_t eb = 0;
+  const int nsh = depth > 0 ? w.counts[kCntSh + depth - 1] : 0;
+  const int next = depth < c.max_depth ? w.counts[kCntExt + depth] : 0;
+  const int *q = w.queue[depth & 1];
+  const int total = nsh + next;
+  int *fetch = w.counts + kCntFetchT + depth;
+  for (;;) {
+    const int base = warp_fetch(fetch);
+    if (base >= total) break;
+    const int i = base + (threadIdx.x & 31);
+    if (i < nsh) {
+      const float4 o = w.sq_origin[i], d = w.sq_dir[i];
+      const int4 m = w.sq_meta[i];
+      ShadowQuery sq;
+      sq.origin = xyz(o);
+      sq.max_dist = o.w;
+      sq.dir = xyz(d);
+      sq.contrib = d.w;
+      sq.light_slot = m.y;
+      sq.vol = m.z;
+      const int band = m.w & 0xff, dep_band = m.w >> 8;
+      ShadowState ss;
+      ss.pos = sq.origin;
+      ss.total = 1.f;
+      ss.traveled = 0.f;
+      ss.vol = sq.vol;
+      ss.seg = 0;
+      for (;;) {
+        const Hit h = trace_closest(s, ss.pos, sq.dir, c.eps, eb);
+        if (shadow_segment(s, c, sq, h, band, ss)) break;
+      }
+      if (ss.total > 1e-6f) deposit(f, m.x, dep_band, sq.contrib * ss.total);
+    } else if (i < total) {
+      const int pid = q[i - nsh];
+      const float4 pt = w.pos_thr[pid], ds = w.dir_spdf[pid];
+      const Hit h = trace_closest(s, xyz(pt), xyz(ds), c.eps, eb);
+      w.hit[pid] = make_float4(h.t, h.u, h.v, __int_as_float(h.slot));
+    }
+  }
+  if (eb) atomicOr(err, eb);
+}
+
+// material key of a queued path for the shading sort (num_materials = miss)
+__device__ __forceinline__ int shade_key(const DevScene &s, const WaveBuffers &w, int pid, int nkeys) {
+  const int slot = __float_as_int(w.hit[pid].w);
+  int key = slot >= 0 ? __float_as_int(__ldg(s.tri + 3 * (size_t)slot + 1).w) : s.num_materials;
+  return key < nkeys ? key : nkeys - 1;
+}
+
+__global__ void k_sort_count(DevScene s, DevConfig c, int depth, WaveBuffers w, int nkeys) {
+  __shared__ int hist[kMaxKeys];
+  for (int k = threadIdx.x; k < nkeys; k += blockDim.x) hist[k] = 0;
+  __syncthreads();
+  const int n = w.counts[kCntExt + depth];
+  const int *q = w.queue[depth & 1];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    atomicAdd(&hist[shade_key(s, w, q[i], nkeys)], 1);
+  __syncthreads();
+  for (int k = threadIdx.x; k < nkeys; k += blockDim.x)
+    if (hist[k]) atomicAdd(&w.key_hist[k], hist[k]);
+}
+
+__global__ void k_sort_scan(WaveBuffers w, int nkeys) {
+  if (threadIdx.x == 0) {
+    int run = 0;
+    for (int k = 0; k < nkeys; ++k) {
+      const int v = w.key_hist[k];
+      w.key_hist[kMaxKeys + k] = run;  // running insert position
+      w.key_hist[k] = 0;               // cleared for the next depth
+      run += v;
+    }
+  }
+}
+
+__global__ void k_sort_scatter(DevScene s, DevConfig c, int depth, WaveBuffers w, int nkeys) {
+  const int n = w.counts[kCntExt + depth];
+  const int *q = w.queue[depth & 1];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int pid = q[i];
+    const int pos = atomicAdd(&w.key_hist[kMaxKeys + shade_key(s, w, pid, nkeys)], 1);
+    w.sorted[pos] = pid;
+  }
+}
+
+__global__ void __launch_bounds__(128) k_shade(DevScene s, DevConfig c, uint32_t pass, int band, int depth,
+                                               Film f, WaveBuffers w, int use_sorted) {
+  const int n = w.counts[kCntExt + depth];
+  const int *q = use_sorted ? w.sorted : w.queue[depth & 1];
+  int *qn = w.queue[(depth + 1) & 1];
+  int *fetch = w.counts + kCntFetchS + depth;
+  for (;;) {
+    const int base = warp_fetch(fetch);
+    if (base >= n) break;
+    const int i = base + (threadIdx.x & 31);
+    bool cont = false, nee = false;
+    int pid = -1, pix = -1, dep_band = 0;
+    ShadowQuery sq;
+    PathState p;
+    Rng rng;
+    if (i < n) {
+      pid = q[i];
+      const float4 pt = w.pos_thr[pid], ds = w.dir_spdf[pid];
+      const int4 m = w.meta[pid];
+      const float4 hh = w.hit[pid];
+      pix = m.x;
+      p.pos = xyz(pt);
+      p.thr = pt.w;
+      p.dir = xyz(ds);
+      p.spdf = ds.w;
+      p.active = m.y & 0xff;
+      p.active_px = (m.y >> 8) & 0xff;
+      p.plen = (m.y >> 16) & 0xffff;
+      p.vol = m.z;
+      rng.init(c.seed, pass, (uint32_t)m.x, c.scene_id, (uint32_t)m.w);
+      Hit h;
+      h.t = hh.x;
+      h.u = hh.y;
+      h.v = hh.z;
+      h.slot = __float_as_int(hh.w);
+      const VolEvent ev = volume_event(s, c, p, h, rng);
+      if (ev.travel >= 0.f) {
+        p.pos = p.pos + p.dir * ev.travel;
+        p.thr *= ev.est;
+        bool done = false;
+        float indirect = 0.f;
+        if (ev.action == 1) {
+          const Mat sm = get_mat(s, c.B, ev.hit_mat, band);
+          if (sm.surf_emis) {
+            indirect = emitter_hit(s, c, p, ev, sm.emission);
+            done = true;
+          } else {
+            nee = nee_setup(s, c, p, band, ev.snormal, ev.hit_mat, rng, sq);
+          }
+        } else {
+          nee = nee_setup(s, c, p, band, ev.snormal, -1, rng, sq);
+        }
+        sq.band = p.active;
+        if (ev.action == 1 && !done) {
+          p.plen++;
+          const SurfEvent se = scatter_surface(s, c, p, ev, rng);
+          apply_surface(c, p, ev, se);
+        } else if (ev.action == 2) {
+          p.dir = ev.dir;
+          p.plen++;
+        } else if (ev.action == 3) {
+          p.dir = ev.dir;
+          p.active = ev.new_wl;
+          p.active_px = ev.new_wl;
+          p.plen++;
+        }
+        dep_band = p.active_px;
+        deposit(f, m.x, dep_band, indirect);
+        cont = !done && depth + 1 < c.max_depth && p.thr != 0.f;
+        if (cont) {
+          w.pos_thr[pid] = make_float4(p.pos.x, p.pos.y, p.pos.z, p.thr);
+          w.dir_spdf[pid] = make_float4(p.dir.x, p.dir.y, p.dir.z, p.spdf);
+          w.meta[pid] = make_int4(m.x, p.active | (p.active_px << 8) | (p.plen << 16), p.vol, (int)rng.n);
+        }
+      }
+    }
+    const int sslot = warp_append(w.counts + kCntSh + depth, nee);
+    if (nee) {
+      w.sq_origin[sslot] = make_float4(sq.origin.x, sq.origin.y, sq.origin.z, sq.max_dist);
+      w.sq_dir[sslot] = make_float4(sq.dir.x, sq.dir.y, sq.dir.z, sq.contrib);
+      w.sq_meta[sslot] = make_int4(pix, sq.light_slot, sq.vol, sq.band | (dep_band << 8));
+    }
+    const int qslot = warp_append(w.counts + kCntExt + depth + 1, cont);
+    if (cont) qn[qslot] = pid;
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_wave_pass(const DevScene &s, const DevConfig &c, uint32_t pass, int band, Film f,
+                             const WaveBuffers &w, uint32_t *err, int grid, int block, int sort_keys,
+                             cudaStream_t st) {
+  if (c.max_depth > kMaxDepth) return cudaErrorInvalidValue;
+  cudaError_t e = cudaMemsetAsync(w.counts, 0, kCntTotal * sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  const int npix = c.W * c.H;
+  const int gen_grid = (npix + 255) / 256;
+  k_generate<<<gen_grid, 256, 0, st>>>(s, c, pass, band, w);
+  const int nkeys = sort_keys ? (s.num_materials + 1 < kMaxKeys ? s.num_materials + 1 : kMaxKeys) : 0;
+  if (nkeys) {
+    e = cudaMemsetAsync(w.key_hist, 0, 2 * kMaxKeys * sizeof(int), st);
+    if (e != cudaSuccess) return e;
+  }
+  for (int d = 0; d < c.max_depth; ++d) {
+    k_trace<<<grid, block, 0, st>>>(s, c, d, f, w, err);
+    if (nkeys) {
+      k_sort_count<<<grid, 256, 0, st>>>(s, c, d, w, nkeys);
+      k_sort_scan<<<1, 32, 0, st>>>(w, nkeys);
+      k_sort_scatter<<<grid, 256, 0, st>>>(s, c, d, w, nkeys);
+    }
+    k_shade<<<grid, block, 0, st>>>(s, c, pass, band, d, f, w, nkeys ? 1 : 0);
+  }
+  // the last depth's shadow queries
+  if (c.max_depth > 0) k_trace<<<grid, block, 0, st>>>(s, c, c.max_depth, f, w, err);
+  return cudaGetLastError();
+}
+
+}  // namespace ts

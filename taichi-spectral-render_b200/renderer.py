@@ -1,0 +1,322 @@
+"""Renderer: the reference's render API on top of libspectral.so.
+
+Method names follow the Taichi kernels of main.py so that the reference's
+application loop (main.py:1826-1840) ports line for line:
+
+    r = Renderer(create_scene(), RenderConfig(), eems=..., cmf=cs.cmf)
+    r.clear_pixel_space()
+    total_samples, blocks = 0, 0
+    while total_samples < r.config.samples_per_pixel:
+        total_samples += 1
+        r.cast_rays((total_samples - 1) % r.config.bands, blocks)
+        if total_samples % r.config.bands == 0:
+            blocks += 1
+            r.average_and_reset_block(blocks)
+            rgb = r.color_rays()
+
+Device memory and streams come from PyTorch (the library itself allocates its
+film and scene buffers and takes the current torch stream).  Nothing here
+computes on the CPU: every render call is a CUDA launch through the C ABI.
+"""
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from .scene import compile_scene
+
+
+@dataclass
+class RenderConfig:
+    """Render constants of main.py:11-35 (reference defaults)."""
+    width: int = 400                # RENDER_WIDTH = IMAGE_WIDTH // RESOLUTION_SCALE
+    height: int = 400
+    bands: int = 25                 # SPECTRAL_BANDS
+    lambda_min: float = 10.0        # WAVELENGTH_MIN [nm]
+    lambda_max: float = 1210.0      # WAVELENGTH_MAX [nm]
+    max_path_length: int = 7        # MAX_PATH_LENGTH
+    scatter_bounces: int = 5        # SCATTER_BOUNCES
+    epsilon: float = 1e-4           # EPSILON
+    escape: float = 1e2             # ESCAPE
+    aspect_ratio: float = 1.0       # ASPECT_RATIO
+    fov_scale: float = 1.0          # 1 = the reference camera (half-FOV atan(1/2))
+    samples_per_pixel: int = 7000   # SAMPLES_PER_PIXEL
+    exposure: float = 1.0           # EXPOSURE
+    gamma: float = 2.0              # GAMMA
+    image_width: int = 800          # IMAGE_WIDTH (display resolution of color_rays)
+    image_height: int = 800
+    seed: int = 0
+    scene_id: int = 0
+    kernel: str = "wavefront"       # "wavefront" or "mega" (plain single-scene megakernel)
+    block_size: int = 0
+    blocks_per_sm: int = 0
+    sort_keys: int = 0
+    device: int = 0
+
+    @property
+    def wavelength_step(self):
+        return (self.lambda_max - self.lambda_min) / (self.bands - 1) if self.bands > 1 else 0.0
+
+    def wavelengths(self):
+        return np.linspace(self.lambda_min, self.lambda_max, self.bands)
+
+    def to_c(self):
+        c = _lib.TsConfig()
+        c.width, c.height, c.bands = self.width, self.height, self.bands
+        c.lambda_min_nm, c.lambda_max_nm = self.lambda_min, self.lambda_max
+        c.max_path_length, c.scatter_bounces = self.max_path_length, self.scatter_bounces
+        c.epsilon, c.escape = self.epsilon, self.escape
+        c.aspect_ratio, c.fov_scale = self.aspect_ratio, self.fov_scale
+        c.seed, c.scene_id, c.device = self.seed & 0xFFFFFFFF, self.scene_id & 0xFFFFFFFF, self.device
+        c.kernel = {"mega": _lib.KERNEL_MEGA, "wavefront": _lib.KERNEL_WAVEFRONT}[self.kernel]
+        c.block_size, c.blocks_per_sm, c.sort_keys = self.block_size, self.blocks_per_sm, self.sort_keys
+        return c
+
+
+def fov_scale_for(vertical_fov_degrees):
+    """fov_scale giving a vertical field of view (the reference's is 2*atan(1/2))."""
+    return 2.0 * np.tan(np.radians(vertical_fov_degrees) / 2.0)
+
+
+class _CudaArray:
+    """Zero-copy view of a device buffer owned by the library context."""
+
+    def __init__(self, ptr, shape, typestr):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr, "data": (int(ptr), False),
+                                         "version": 3, "strides": None}
+
+
+def _stream():
+    import torch
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+class Renderer:
+    """One scene on one GPU (a libspectral context)."""
+
+    def __init__(self, scene_dict, config=None, eems=None, cmf=None, bvh=None, bvh_params=None, exact=None,
+                 cmf_scale=None):
+        import torch
+        if not torch.cuda.is_available():
+            raise RuntimeError("spectral_b200.Renderer needs a CUDA device (there is no CPU fallback)")
+        self.config = config or RenderConfig()
+        self.lib = _lib.load()
+        self._ctx = ctypes.c_void_p()
+        _lib.check(self.lib.ts_create(ctypes.byref(self.config.to_c()), ctypes.byref(self._ctx)))
+        self.device = torch.device("cuda", self.config.device)
+        self.total_samples = 0
+        self.num_blocks_completed = 0
+        self._cam = None
+        self.compiled = None
+        # the reference's normalisation: step / (sum_k cmf_y * step) (main.py:392-394, 1620)
+        self.cmf_scale = cmf_scale
+        self.setup_scene(scene_dict, eems=eems, cmf=cmf, bvh=bvh, bvh_params=bvh_params, exact=exact)
+
+    # ---------------------------------------------------------------- lifecycle
+    def close(self):
+        if self._ctx:
+            self.lib.ts_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, status):
+        _lib.check(status, self._ctx)
+
+    # ---------------------------------------------------------------- scene
+    def setup_scene(self, scene_dict, eems=None, cmf=None, bvh=None, bvh_params=None, exact=None):
+        """setup_scene + build_bvh (main.py:437-631): flatten, build the BVH, upload."""
+        cs = compile_scene(scene_dict, self.config.bands, eems=eems, cmf=cmf, bvh=bvh, bvh_params=bvh_params,
+                           exact=exact)
+        d = cs.desc()
+        self._check(self.lib.ts_upload_scene(self._ctx, ctypes.byref(d)))
+        self.compiled = cs
+        if self.cmf_scale is None:
+            ysum = float(np.sum(cs.cmf.astype(np.float64)[:, 1])) * self.config.wavelength_step
+            self.cmf_scale = self.config.wavelength_step / ysum if ysum > 0 else 0.0
+        cam = scene_dict.get("camera")
+        if cam is not None:
+            self.update_camera(cam["origin"], cam["lookat"], cam["up"])
+
+    def scene_info(self):
+        info = _lib.TsSceneInfo()
+        self._check(self.lib.ts_scene_info_get(self._ctx, ctypes.byref(info)))
+        return {k: getattr(info, k) for k, _ in info._fields_}
+
+    def tri_perm(self):
+        """slot -> original triangle index of the uploaded BVH order."""
+        n = self.compiled.num_tris
+        out = np.zeros(n, np.int32)
+        self._check(self.lib.ts_get_tri_perm(self._ctx, out.ctypes.data_as(_lib.I32P)))
+        return out
+
+    # ---------------------------------------------------------------- camera
+    def update_camera(self, origin=None, lookat=None, up=None):
+        """update_camera (main.py:633-640); arguments replace the stored ones."""
+        o, l, u = self._cam or ([0.0, 0.0, 3.5], [0.0, 0.0, -1.0], [0.0, 1.0, 0.0])
+        o = o if origin is None else origin
+        l = l if lookat is None else lookat
+        u = u if up is None else up
+        self._cam = (list(map(float, o)), list(map(float, l)), list(map(float, u)))
+        arr = lambda v: (ctypes.c_float * 3)(*v)
+        self._check(self.lib.ts_set_camera(self._ctx, arr(self._cam[0]), arr(self._cam[1]), arr(self._cam[2])))
+
+    # ---------------------------------------------------------------- render
+    def cast_rays(self, current_sample_in_block, block_index=0, pass_idx=None):
+        """One sample pass at band ``current_sample_in_block`` (main.py:1502-1590).
+
+        pass_idx picks the random stream; by default it is the number of passes
+        rendered since the last clear, so a cleared renderer replays the same
+        sample sequence (common random numbers)."""
+        if pass_idx is None:
+            pass_idx = self.total_samples
+        self._check(self.lib.ts_render_pass(self._ctx, int(pass_idx) & 0xFFFFFFFF, int(current_sample_in_block),
+                                            _stream()))
+        self.total_samples += 1
+
+    def average_and_reset_block(self, num_blocks_completed):
+        """main.py:1592-1607 (FP64 running mean plus the per-cell sum of squares)."""
+        self._check(self.lib.ts_accumulate_block(self._ctx, int(num_blocks_completed), _stream()))
+        self.num_blocks_completed = int(num_blocks_completed)
+
+    def clear_pixel_space(self):
+        """main.py:1661-1674."""
+        self._check(self.lib.ts_reset(self._ctx, _stream()))
+        self.total_samples = 0
+        self.num_blocks_completed = 0
+
+    def render(self, samples=None, callback=None):
+        """The pass/block cadence of main.py:1826-1837 for ``samples`` passes."""
+        samples = self.config.samples_per_pixel if samples is None else samples
+        B = self.config.bands
+        for _ in range(samples):
+            band = self.total_samples % B
+            self.cast_rays(band, self.num_blocks_completed)
+            if self.total_samples % B == 0:
+                self.average_and_reset_block(self.num_blocks_completed + 1)
+                if callback is not None:
+                    callback(self)
+        return self
+
+    # ---------------------------------------------------------------- film views
+    def _film(self, which):
+        import torch
+        ptr = ctypes.POINTER(ctypes.c_double)()
+        n = ctypes.c_size_t()
+        self._check(self.lib.ts_film_buffer(self._ctx, which, ctypes.byref(ptr), ctypes.byref(n)))
+        c = self.config
+        addr = ctypes.cast(ptr, ctypes.c_void_p).value
+        return torch.as_tensor(_CudaArray(addr, (c.bands, c.height, c.width), "<f8"), device=self.device)
+
+    @property
+    def block_film(self):
+        """Current block's per-band sums, [B][H][W] float64 (device view)."""
+        return self._film(_lib.FILM_BLOCK)
+
+    @property
+    def mean_film(self):
+        """Running mean over completed blocks, [B][H][W] float64 (device view)."""
+        return self._film(_lib.FILM_MEAN)
+
+    @property
+    def m2_film(self):
+        """Sum over blocks of the squared block values, [B][H][W] float64 (device view)."""
+        return self._film(_lib.FILM_M2)
+
+    @property
+    def spectral_accumulator(self):
+        """The reference's spectral_accumulator[i, j, k] layout (a [W][H][B] view)."""
+        return self.mean_film.permute(2, 1, 0)
+
+    @property
+    def block_accumulator(self):
+        return self.block_film.permute(2, 1, 0)
+
+    def standard_error(self):
+        """Per-cell standard error of the block mean, [B][H][W] float64."""
+        n = self.num_blocks_completed
+        if n < 2:
+            raise ValueError("need at least two completed blocks")
+        mean, m2 = self.mean_film, self.m2_film
+        var = (m2 / n - mean * mean).clamp_min(0.0) * (n / (n - 1))
+        return (var / n).sqrt()
+
+    # ---------------------------------------------------------------- resolve
+    def resolve_xyz(self, out=None):
+        """XYZ at render resolution, [H][W][3] float32 (XYZ half of color_rays)."""
+        import torch
+        c = self.config
+        if out is None:
+            out = torch.empty((c.height, c.width, 3), dtype=torch.float32, device=self.device)
+        self._check(self.lib.ts_resolve_xyz(self._ctx, float(self.cmf_scale), ctypes.c_void_p(out.data_ptr()),
+                                            _stream()))
+        return out
+
+    def resolve_xyz_host(self, out=None):
+        """Same, into a (pinned) host array; the stream is synchronised."""
+        c = self.config
+        if out is None:
+            out = np.empty((c.height, c.width, 3), np.float32)
+        self._check(self.lib.ts_resolve_xyz_host(self._ctx, float(self.cmf_scale),
+                                                 out.ctypes.data_as(_lib.F32P), _stream()))
+        return out
+
+    def color_rays(self, xyz_to_rgb=None, out=None):
+        """color_rays (main.py:1609-1629): [image_height][image_width][3] float32 device image."""
+        import torch
+        c = self.config
+        if xyz_to_rgb is None:
+            from .spectral_data import srgb_xyz_to_rgb
+            xyz_to_rgb = srgb_xyz_to_rgb()
+        m = (ctypes.c_float * 9)(*np.asarray(xyz_to_rgb, np.float64).reshape(9).tolist())
+        if out is None:
+            out = torch.empty((c.image_height, c.image_width, 3), dtype=torch.float32, device=self.device)
+        self._check(self.lib.ts_resolve_rgb(self._ctx, float(self.cmf_scale), m, c.exposure, c.gamma,
+                                            c.image_width, c.image_height, ctypes.c_void_p(out.data_ptr()),
+                                            _stream()))
+        return out
+
+    def visualize_normals(self, out=None):
+        """Geometry mode (main.py:1631-1659): shading normal * 0.5 + 0.5, [H][W][3]."""
+        import torch
+        c = self.config
+        if out is None:
+            out = torch.empty((c.height, c.width, 3), dtype=torch.float32, device=self.device)
+        self._check(self.lib.ts_render_normals(self._ctx, ctypes.c_void_p(out.data_ptr()), _stream()))
+        return out
+
+    # ---------------------------------------------------------------- queries
+    def trace(self, rays, mode="fast"):
+        """Closest hit of [n][6] rays (a torch CUDA tensor) -> (tri, t, u, v).
+
+        tri is the ORIGINAL triangle index (-1 on a miss), t = 1e9 on a miss.
+        mode "reference_order" walks the tree exactly like the reference's trace.
+        """
+        import torch
+        rays = rays.to(device=self.device, dtype=torch.float32).contiguous()
+        n = rays.shape[0]
+        tri = torch.empty(n, dtype=torch.int32, device=self.device)
+        t = torch.empty(n, dtype=torch.float32, device=self.device)
+        u = torch.empty(n, dtype=torch.float32, device=self.device)
+        v = torch.empty(n, dtype=torch.float32, device=self.device)
+        m = {"fast": _lib.TRACE_FAST, "reference_order": _lib.TRACE_REFERENCE_ORDER}[mode]
+        p = lambda x: ctypes.c_void_p(x.data_ptr())
+        self._check(self.lib.ts_trace_batch(self._ctx, p(rays), n, m, p(tri), p(t), p(u), p(v), _stream()))
+        return tri, t, u, v
+
+    def check_device(self):
+        """Raise if a kernel reported an error bit since the last check (synchronises)."""
+        bits = ctypes.c_uint32()
+        self._check(self.lib.ts_check_device(self._ctx, ctypes.byref(bits)))
+        return bits.value
