@@ -1,0 +1,334 @@
+"""Benchmark: spectral path-tracing sample passes on the large-mesh workload.
+
+One step = one sample pass (cast_rays) over every pixel of the workload at
+one wavelength band: 1024x1024 paths of depth <= 12 through a 2.59M-triangle
+scene (1024^2-vertex heightfield + 500k-triangle displaced sphere, GGX
+conductors, 8 emissive quads, 25 bands over 380-740 nm).  The metric is
+Mpaths/s (one path = one pixel x one band-pass, the reference's unit).
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+                  [--kernel mega|wavefront] [--workload terrain|box|volume]
+
+--impl reference times the reference's CPU path: the FP32 restatement of its
+estimator (oracle/, OpenMP over all host threads), since the reference's own
+Taichi kernels cannot be installed here.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# algorithmic bytes of one unit of work, for the roofline (layouts in csrc/common.cuh)
+BYTES_NODE = 64      # one two-child BVH node (two child boxes + links)
+BYTES_TRI = 48       # one triangle test (v0, e1, e2 as float4)
+BYTES_HIT = 48       # shading normals of a resolved hit (3 float4)
+BYTES_MAT_VERTEX = 8 * 32  # material lookups per path vertex (8 x two float4)
+BYTES_DEPOSIT = 16   # FP64 read-modify-write of a film cell
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=300)
+    p.add_argument("--warmup", type=int, default=10)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--kernel", default="mega", choices=["mega", "wavefront"])
+    p.add_argument("--workload", default="terrain", choices=["terrain", "box", "volume"])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def workload(name):
+    from spectral_b200 import configs
+    if name == "terrain":
+        scene, cfg, ex = configs.terrain_scene()
+        desc = ("terrain: 1024^2-vertex heightfield (2.09M tris, 6-octave value noise) + 500k-tri displaced "
+                "sphere, GGX conductors, 8 emissive quads; 1024x1024, depth 12, 25 bands 380-740 nm, 256 spp")
+    elif name == "box":
+        scene, cfg, ex = configs.box_scene()
+        desc = "box: 12-tri box + 2048-tri GGX dielectric sphere + quad light; 256x256, depth 8, 25 bands, 64 spp"
+    else:
+        scene, cfg, ex = configs.volume_scene()
+        desc = ("volume: box + 20k-tri HG medium (g 0.7) + fluorescent wall; 512x512, depth 32, 25 bands, "
+                "512 spp")
+    return scene, cfg, ex, desc
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", str(rank)))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id=None):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        cmd = ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "100"]
+        if self.gpu_id is not None:
+            cmd += ["-i", str(self.gpu_id)]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[5:9], parts[4]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i, v in enumerate(r[2]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def gpu_uuid(dev):
+    import torch
+    try:
+        u = torch.cuda.get_device_properties(dev).uuid
+        return f"GPU-{u}"
+    except Exception:
+        return None
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "of measured"
+    return 6650.0, "of fallback"
+
+
+def profiled_traffic(kernel, workload_name):
+    """DRAM bytes per launch from the committed ncu summary (None if not captured)."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(path):
+        return None
+    d = json.load(open(path))
+    e = d.get(f"{workload_name}:{kernel}")
+    return None if e is None else float(e["dram_bytes_per_launch"])
+
+
+def cpu_oracle_rate(comp, bvh, scene, cfg, seconds, nthreads=0, passes=None):
+    """Paths/s of the FP32 oracle on a pixel sample sized for ~``seconds``."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import orc
+    osc = orc.oracle_scene(comp, bvh, scene["camera"])
+    ocfg = orc.oracle_config(cfg)
+    npix = cfg.width * cfg.height
+    rng = np.random.default_rng(123)
+    n = 1024
+    pix = rng.choice(npix, min(n, npix), replace=False).astype(np.int32)
+    t = time.perf_counter()
+    orc.render_pass(osc, ocfg, 0, 12, pix, nthreads=nthreads)
+    dt = max(time.perf_counter() - t, 1e-6)
+    rate = len(pix) / dt
+    n = int(min(npix, max(1024, rate * seconds)))
+    pix = rng.choice(npix, n, replace=False).astype(np.int32)
+    t = time.perf_counter()
+    _, st = orc.render_pass(osc, ocfg, 1, 12, pix, nthreads=nthreads)
+    dt = time.perf_counter() - t
+    threads = nthreads if nthreads > 0 else (os.cpu_count() or 1)
+    return n / dt, n, dt, threads, st
+
+
+def bench_reference(args):
+    """CPU arm: the reference estimator (oracle restatement) on all host threads."""
+    import numpy as np
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    import spectral_b200 as sb
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import orc
+    scene, cfg, ex, desc = workload(args.workload)
+    comp = sb.compile_scene(scene, cfg.bands, eems=ex["eems"], cmf=ex["cmf"])
+    bvh = sb._lib.build_bvh_host(comp.tris["v0"], comp.tris["v1"], comp.tris["v2"])
+    osc = orc.oracle_scene(comp, bvh, scene["camera"])
+    ocfg = orc.oracle_config(cfg)
+    npix = cfg.width * cfg.height
+    rng = np.random.default_rng(7)
+    # size each step so that the whole run takes ~2 minutes
+    pix = rng.choice(npix, 1024, replace=False).astype(np.int32)
+    t = time.perf_counter()
+    orc.render_pass(osc, ocfg, 0, 0, pix)
+    rate = 1024 / max(time.perf_counter() - t, 1e-6)
+    per_step = int(min(npix, max(256, rate * min(0.5, 120.0 / max(1, args.steps + args.warmup)))))
+    for w in range(args.warmup):
+        pix = rng.choice(npix, per_step, replace=False).astype(np.int32)
+        orc.render_pass(osc, ocfg, w, w % cfg.bands, pix)
+    total = 0.0
+    for k in range(args.steps):
+        pix = rng.choice(npix, per_step, replace=False).astype(np.int32)
+        t = time.perf_counter()
+        orc.render_pass(osc, ocfg, args.warmup + k, k % cfg.bands, pix)
+        total += time.perf_counter() - t
+    mpaths = per_step * args.steps / total / 1e6
+    threads = os.cpu_count() or 1
+    sample = f"{per_step} random pixels of one band-pass per step (of {npix} per full pass)"
+    line = {"impl": "reference", "metric": "Mpaths/s", "value": mpaths, "unit": "Mpaths/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded procedural scene)",
+            "config": {"workload": desc, "paths_per_step": per_step, "bvh": "library binned-SAH tree in the "
+                       "reference layout, traversed in the reference order without distance culling"},
+            "cpu_baseline": {"value": mpaths, "unit": "Mpaths/s", "cores": threads, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": mpaths, "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def bench_ours(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import spectral_b200 as sb
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    scene, cfg, ex, desc = workload(args.workload)
+    cfg.kernel = args.kernel
+    cfg.device = local
+    comp = sb.compile_scene(scene, cfg.bands, eems=ex["eems"], cmf=ex["cmf"])
+    bvh = sb._lib.build_bvh_host(comp.tris["v0"], comp.tris["v1"], comp.tris["v2"])
+    r = sb.Renderer(scene, cfg, eems=ex["eems"], cmf=ex["cmf"], bvh=bvh)
+    B = cfg.bands
+    paths_per_step = cfg.width * cfg.height
+    base_pass = rank * (args.warmup + args.steps + 8) * 4  # disjoint random streams per rank
+
+    # warm-up, then one counted pass (work counters for the roofline's algorithmic bytes)
+    for w in range(args.warmup):
+        r.cast_rays(w % B, pass_idx=base_pass + w)
+    work = r.cast_rays_counted(12, pass_idx=base_pass + args.warmup)
+    torch.cuda.synchronize()
+    bytes_per_path = (BYTES_NODE * work["node_visits"] + BYTES_TRI * work["tri_tests"] + BYTES_HIT * work["hits"]
+                      + BYTES_MAT_VERTEX * work["vertices"] + BYTES_DEPOSIT * work["deposits"]) / work["paths"]
+
+    # ---- timed region: K passes, device time, max over ranks
+    sampler = ClockSampler(gpu_uuid(local))
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for k in range(args.steps):
+        r.cast_rays(k % B, pass_idx=base_pass + args.warmup + 1 + k)
+    e1.record()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    if world > 1:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * args.steps * paths_per_step / (ms_max * 1e-3) / 1e6
+    bits = r.check_device()
+
+    # ---- end to end through the public API with host buffers: camera in,
+    # resolved XYZ image out (pinned), every step
+    out = torch.empty((cfg.height, cfg.width, 3), dtype=torch.float32, pin_memory=True).numpy()
+    cam = scene["camera"]
+    e2e_steps = max(10, args.steps // 3)
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record()
+    for k in range(e2e_steps):
+        r.update_camera(cam["origin"], cam["lookat"], cam["up"])
+        r.cast_rays(k % B, pass_idx=base_pass + 7 * (args.steps + 1) + k)
+        r.resolve_xyz_host(out)
+    f1.record()
+    torch.cuda.synchronize()
+    e2e_ms = f0.elapsed_time(f1)
+    t2 = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t2, op=dist.ReduceOp.MAX)
+    e2e_value = world * e2e_steps * paths_per_step / (float(t2.item()) * 1e-3) / 1e6
+
+    launches_per_step = 1 if args.kernel == "mega" else 2 + 2 * cfg.max_path_length
+    peak, peak_src = measured_peak()
+    step_s = ms_max * 1e-3 / args.steps
+    achieved = bytes_per_path * paths_per_step / step_s / 1e9
+    traffic = profiled_traffic(args.kernel, args.workload)
+
+    line = {"metric": "Mpaths/s", "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded procedural scene; no dataset)",
+            "config": {"workload": desc, "kernel": args.kernel, "paths_per_step": paths_per_step,
+                       "spp": ex["spp"], "passes_for_spp": cfg.samples_per_pixel,
+                       "l2": "inputs larger than L2: scene %.0f MB + film %.0f MB > 126 MB L2; no flush"
+                             % ((r.scene_info()["device_bytes"] - 3 * paths_per_step * B * 8) / 1e6,
+                                paths_per_step * B * 8 / 1e6),
+                       "parallelism": f"{world} GPU(s), disjoint sample passes per GPU"},
+            "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": 36,
+                    "d2h_bytes_per_step": int(out.nbytes),
+                    "what": "Renderer.update_camera + cast_rays + resolve_xyz_host (pinned host XYZ image) per "
+                            "step, through the C ABI"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "k_render_mega" if args.kernel == "mega" else "wavefront pass",
+                         "bytes_per_path": bytes_per_path, "peak_source": peak_src,
+                         "work_per_path": {k: v / work["paths"] for k, v in work.items() if k != "paths"}},
+            "gpu_launches": launches_per_step * args.steps,
+            "clocks": clocks, "device_error_bits": bits}
+
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, n, dt, threads, st = cpu_oracle_rate(comp, bvh, scene, cfg, seconds=12.0)
+        line["cpu_baseline"] = {"value": rate / 1e6, "unit": "Mpaths/s", "cores": threads, "kind": "port",
+                                "sample": f"{n} random pixels of one band-pass ({dt:.1f} s, FP32 oracle, "
+                                          f"reference traversal order)"}
+    r.close()
+    if world > 1:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    a = parse()
+    if a.impl == "reference":
+        bench_reference(a)
+    else:
+        bench_ours(a)

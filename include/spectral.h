@@ -53,7 +53,7 @@ typedef struct {
   uint32_t scene_id;             /* Philox counter word 2 (distinguishes scenes of a batch) */
   int32_t device;                /* CUDA device ordinal */
   int32_t kernel;                /* TS_KERNEL_MEGA or TS_KERNEL_WAVEFRONT */
-  int32_t block_size;            /* threads per block of the render kernels (0 = default) */
+  int32_t block_size;            /* threads per block of the render kernels, 32..256 (0 = 128) */
   int32_t blocks_per_sm;         /* persistent grid = SMs * blocks_per_sm (0 = default) */
   int32_t sort_keys;             /* wavefront: sort shading queue by material (0 = off) */
 } ts_config;
@@ -120,6 +120,13 @@ ts_status ts_set_camera(ts_ctx *ctx, const float origin[3], const float lookat[3
  * pass_idx selects the random stream (Philox key word 1); band is the pass's
  * wavelength index (current_sample_in_block).  Deposits into TS_FILM_BLOCK. */
 ts_status ts_render_pass(ts_ctx *ctx, uint32_t pass_idx, int32_t band, void *stream);
+
+/* The same pass rendered by the plain megakernel with work counters (used to
+ * derive algorithmic bytes per path).  work[0..6] = paths, path vertices,
+ * traversals, BVH node visits, triangle tests, hits resolved, film deposits;
+ * work[7] unused.  Deposits into TS_FILM_BLOCK like ts_render_pass; the
+ * stream is synchronised. */
+ts_status ts_render_pass_counted(ts_ctx *ctx, uint32_t pass_idx, int32_t band, void *stream, uint64_t work[8]);
 
 /* ---- film (average_and_reset_block, clear_pixel_space, main.py:1592-1607, 1661-1674) */
 ts_status ts_accumulate_block(ts_ctx *ctx, int32_t num_blocks_completed, void *stream);

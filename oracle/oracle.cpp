@@ -940,6 +940,25 @@ void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t ou
   philox_block(ctr, key, out);
 }
 
+double orc_fresnel(double cos_i, double ni, double ki, double nt, double kt, int32_t use_double) {
+  if (use_double) return fresnel<double>(cos_i, ni, ki, nt, kt);
+  return fresnel<float>((float)cos_i, (float)ni, (float)ki, (float)nt, (float)kt);
+}
+
+double orc_ggx_d(double ndh, double rough, int32_t use_double) {
+  orc_config c{};
+  c.bands = 1;
+  if (use_double) return ggx_d(Ctx<double>(nullptr, &c), ndh, rough);
+  return ggx_d(Ctx<float>(nullptr, &c), (float)ndh, (float)rough);
+}
+
+double orc_hg_eval(double cos_t, double g, int32_t use_double) {
+  orc_config c{};
+  c.bands = 1;
+  if (use_double) return hg_eval(Ctx<double>(nullptr, &c), cos_t, g);
+  return hg_eval(Ctx<float>(nullptr, &c), (float)cos_t, (float)g);
+}
+
 void orc_trace(const orc_scene *s, const orc_config *c, const float *rays, int32_t n, int32_t *tri,
                float *t, float *u, float *v, int32_t use_double) {
 #ifdef _OPENMP

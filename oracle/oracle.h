@@ -73,6 +73,13 @@ typedef struct {
 /* Philox-4x32-10 block (Salmon et al., SC'11); exposed for the RNG tests. */
 void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 
+/* Single-function known-answer hooks: fresnel_spectral (main.py:925-966),
+ * normaldistrobution_ggx (main.py:900-907), evaluate_henyey_greenstein
+ * (main.py:758-766), in float32 or float64. */
+double orc_fresnel(double cos_i, double ni, double ki, double nt, double kt, int32_t use_double);
+double orc_ggx_d(double ndh, double rough, int32_t use_double);
+double orc_hg_eval(double cos_t, double g, int32_t use_double);
+
 /* Closest hit with the reference traversal (main.py:831-864): explicit stack,
  * right child popped first, no distance culling.  rays: [n][6] (pos, dir).
  * Outputs: tri (reordered index, -1 on miss), t (1e9 on miss), u, v. */

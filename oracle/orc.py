@@ -69,6 +69,13 @@ def lib():
         L.orc_build_bvh_sweep.argtypes = [ctypes.c_int32, F32P, F32P, F32P, ctypes.c_int32, F32P, F32P,
                                           I32P, I32P, I32P, I32P, I32P]
         L.orc_build_bvh_sweep.restype = ctypes.c_int32
+        d = ctypes.c_double
+        L.orc_fresnel.argtypes = [d, d, d, d, d, ctypes.c_int32]
+        L.orc_fresnel.restype = d
+        L.orc_ggx_d.argtypes = [d, d, ctypes.c_int32]
+        L.orc_ggx_d.restype = d
+        L.orc_hg_eval.argtypes = [d, d, ctypes.c_int32]
+        L.orc_hg_eval.restype = d
         _LIB = L
     return _LIB
 
@@ -140,6 +147,18 @@ class Scene:
         self.s = s
 
 
+def fresnel(cos_i, ni, ki, nt, kt, use_double=False):
+    return lib().orc_fresnel(cos_i, ni, ki, nt, kt, int(use_double))
+
+
+def ggx_d(ndh, rough, use_double=False):
+    return lib().orc_ggx_d(ndh, rough, int(use_double))
+
+
+def hg_eval(cos_t, g, use_double=False):
+    return lib().orc_hg_eval(cos_t, g, int(use_double))
+
+
 def trace(scene, cfg, rays, use_double=False):
     rays = _f32(rays).reshape(-1, 6)
     n = rays.shape[0]
@@ -195,3 +214,74 @@ def build_bvh_sweep(v0, v1, v2):
     assert N >= 0
     return dict(node_min=nmin[:N], node_max=nmax[:N], node_left=left[:N], node_right=right[:N],
                 node_num_tris=ntri[:N], node_tri_start=tstart[:N], perm=perm)
+
+
+# ---------------------------------------------------------------- scene bridge
+def camera_basis(origin, lookat, up):
+    """update_camera (main.py:633-640) in float32."""
+    f = np.float32
+    o, l, u = (np.asarray(v, np.float32) for v in (origin, lookat, up))
+
+    def nrm(a):
+        return a / np.sqrt(f(a[0] * a[0]) + f(a[1] * a[1]) + f(a[2] * a[2]))
+
+    def cr(a, b):
+        return np.array([a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]], np.float32)
+
+    w = nrm(o - l)
+    uu = nrm(cr(u, w))
+    v = cr(w, uu)
+    return o, uu, v, w
+
+
+def light_tables(mat_i32, slot_mat, slot_area, bands):
+    """Per-band light CDF over triangle slots, float32 running sums (main.py:590-627)."""
+    slot_area = np.asarray(slot_area, np.float32)
+    lists = [np.nonzero(mat_i32[slot_mat, 1, b])[0] for b in range(bands)]
+    L = max([1] + [len(x) for x in lists])
+    cdf = np.zeros((bands, L), np.float32)
+    idx = np.zeros((bands, L), np.int32)
+    nl = np.zeros(bands, np.int32)
+    area = np.zeros(bands, np.float32)
+    for b, lst in enumerate(lists):
+        nl[b] = len(lst)
+        if not len(lst):
+            continue
+        a = slot_area[lst]
+        tot = np.cumsum(a, dtype=np.float32)[-1]  # sequential float32 sum
+        area[b] = tot
+        cdf[b, :len(lst)] = np.cumsum((a / tot).astype(np.float32), dtype=np.float32)
+        idx[b, :len(lst)] = lst
+    return cdf, idx, nl, area
+
+
+def oracle_scene(compiled, bvh, camera):
+    """Oracle scene matching a GPU upload slot for slot.
+
+    compiled: a CompiledScene of the package (original-order triangles and
+    material tables); bvh: a tree in the reference layout with tri_perm (the
+    same tree given to the GPU), so both sides see the same triangle slots and
+    light CDF order."""
+    perm = np.asarray(bvh["tri_perm"], np.int64)
+    t = compiled.tris
+    arrays = {k: t[k][perm] for k in ("v0", "v1", "v2", "n0", "n1", "n2", "normal", "area", "mat_id")}
+    for k in ("node_min", "node_max", "node_left", "node_right", "node_num_tris", "node_tri_start"):
+        arrays[k] = bvh[k]
+    B = compiled.mat_f32.shape[2]
+    arrays["mat_f32"] = compiled.mat_f32
+    arrays["mat_i32"] = compiled.mat_i32
+    arrays["mat_eem"] = compiled.mat_eem
+    arrays["eem"] = compiled.eem
+    cdf, idx, nl, area = light_tables(compiled.mat_i32, arrays["mat_id"], arrays["area"], B)
+    arrays.update(light_cdf=cdf, light_idx=idx, num_lights=nl, light_area=area)
+    o, u, v, w = camera_basis(camera["origin"], camera["lookat"], camera["up"])
+    arrays.update(cam_origin=o, cam_u=u, cam_v=v, cam_w=w)
+    return Scene(arrays)
+
+
+def oracle_config(cfg, scene_id=0):
+    """Oracle config from a RenderConfig."""
+    return Config(width=cfg.width, height=cfg.height, bands=cfg.bands, lambda_min=cfg.lambda_min,
+                      lambda_max=cfg.lambda_max, epsilon=cfg.epsilon, escape=cfg.escape,
+                      max_path_length=cfg.max_path_length, scatter_bounces=cfg.scatter_bounces,
+                      aspect_ratio=cfg.aspect_ratio, fov_scale=cfg.fov_scale, seed=cfg.seed, scene_id=scene_id)

@@ -72,6 +72,8 @@ SIGNATURES = [
                                          I32P, I32P, I32P, I32P]),
     ("ts_set_camera", ctypes.c_int, [_VP, F32P, F32P, F32P]),
     ("ts_render_pass", ctypes.c_int, [_VP, ctypes.c_uint32, ctypes.c_int32, _VP]),
+    ("ts_render_pass_counted", ctypes.c_int, [_VP, ctypes.c_uint32, ctypes.c_int32, _VP,
+                                              ctypes.POINTER(ctypes.c_uint64)]),
     ("ts_accumulate_block", ctypes.c_int, [_VP, ctypes.c_int32, _VP]),
     ("ts_reset", ctypes.c_int, [_VP, _VP]),
     ("ts_film_buffer", ctypes.c_int, [_VP, ctypes.c_int32, ctypes.POINTER(F64P), ctypes.POINTER(ctypes.c_size_t)]),

@@ -136,7 +136,7 @@ ts_status ts_create(const ts_config *cfg, ts_ctx **out) {
   ts_ctx *c = new ts_ctx();
   c->cfg = k;
   if (c->cfg.block_size <= 0) c->cfg.block_size = 128;
-  c->cfg.block_size = std::min(1024, std::max(32, c->cfg.block_size / 32 * 32));
+  c->cfg.block_size = std::min(ts::kMaxBlock, std::max(32, c->cfg.block_size / 32 * 32));
   cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, k.device);
   ts::DevConfig &d = c->dc;
   d.W = k.width;
@@ -457,6 +457,25 @@ ts_status ts_render_pass(ts_ctx *c, uint32_t pass_idx, int32_t band, void *strea
                                     c->cfg.sort_keys, st),
             "render pass");
   }
+  return TS_OK;
+}
+
+ts_status ts_render_pass_counted(ts_ctx *c, uint32_t pass_idx, int32_t band, void *stream, uint64_t work[8]) {
+  if (!c || !work) return fail(c, TS_ERR_INVALID_ARG, "ts_render_pass_counted: bad argument");
+  if (!c->has_scene) return fail(c, TS_ERR_NO_SCENE, "ts_render_pass_counted: no scene uploaded");
+  if (band < 0 || band >= c->cfg.bands) return fail(c, TS_ERR_INVALID_ARG, "ts_render_pass_counted: band out of range");
+  cudaSetDevice(c->cfg.device);
+  const cudaStream_t st = as_stream(stream);
+  const int bs = c->cfg.block_size;
+  int per_sm = c->cfg.blocks_per_sm;
+  if (per_sm <= 0) per_sm = std::max(1, 2048 / bs);
+  unsigned long long *d_work = reinterpret_cast<unsigned long long *>(c->d_counter + 8);
+  TS_CUDA(c, cudaMemsetAsync(d_work, 0, 8 * sizeof(unsigned long long), st), "counted pass");
+  TS_CUDA(c, ts::launch_render_mega(c->ds, c->dc, pass_idx, band, film_of(c), c->d_counter, c->d_err,
+                                    c->num_sms * per_sm, bs, st, d_work),
+          "counted pass");
+  TS_CUDA(c, cudaMemcpyAsync(work, d_work, 8 * sizeof(uint64_t), cudaMemcpyDeviceToHost, st), "counted pass");
+  TS_CUDA(c, cudaStreamSynchronize(st), "counted pass");
   return TS_OK;
 }
 

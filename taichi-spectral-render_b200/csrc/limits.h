@@ -4,4 +4,5 @@
 namespace ts {
 constexpr int kStackDepth = 64;  // traversal stack entries per ray (bounds the tree depth)
 constexpr int kLeafMax = 16;     // triangles per leaf in the two-child layout (4-bit count)
+constexpr int kMaxBlock = 256;   // largest thread block of the render kernels
 }  // namespace ts

@@ -21,9 +21,16 @@ __device__ __forceinline__ void flush(Film f, int pixel, int band, double dep) {
   }
 }
 
-__global__ void __launch_bounds__(128) k_render_mega(DevScene s, DevConfig c, uint32_t pass, int band, Film f,
-                                                     int *__restrict__ counter, uint32_t *__restrict__ err) {
+// kCount: also count the work (for the roofline's algorithmic bytes):
+// work[0..7] = paths, path vertices, traversals, node visits, triangle tests,
+// surface hits resolved, film deposits, (unused).
+template <bool kCount>
+__global__ void __launch_bounds__(kMaxBlock) k_render_mega(DevScene s, DevConfig c, uint32_t pass, int band, Film f,
+                                                     int *__restrict__ counter, uint32_t *__restrict__ err,
+                                                     unsigned long long *__restrict__ work) {
   const int lane = threadIdx.x & 31;
+  TraceCount tc;
+  uint32_t n_paths = 0, n_vert = 0, n_trace = 0, n_hit = 0, n_dep = 0;
   const int npix = c.W * c.H;
   uint32_t errbits = 0;
   int pix = -1;
@@ -44,6 +51,7 @@ __global__ void __launch_bounds__(128) k_render_mega(DevScene s, DevConfig c, ui
         const int idx = base + __popc(m & ((1u << lane) - 1u));
         if (idx < npix) {
           pix = idx;
+          if (kCount) n_paths++;
           rng.init(c.seed, pass, (uint32_t)idx, c.scene_id);
           camera_ray(s, c, idx % c.W, idx / c.W, rng, p, band);
           k = 0;
@@ -58,11 +66,16 @@ __global__ void __launch_bounds__(128) k_render_mega(DevScene s, DevConfig c, ui
 
     // ---- one path vertex (one iteration of the loop at main.py:1534)
     bool done = false;
-    const Hit h = trace_closest(s, p.pos, p.dir, c.eps, errbits);
+    const Hit h = trace_closest<kCount>(s, p.pos, p.dir, c.eps, errbits, &tc);
     const VolEvent ev = volume_event(s, c, p, h, rng);
+    if (kCount) {
+      n_trace++;
+      n_hit += h.slot >= 0;
+    }
     if (ev.travel < 0.f) {
       done = true;  // escaped
     } else {
+      if (kCount) n_vert++;
       p.pos = p.pos + p.dir * ev.travel;
       p.thr *= ev.est;
       float indirect = 0.f, direct = 0.f;
@@ -87,7 +100,11 @@ __global__ void __launch_bounds__(128) k_render_mega(DevScene s, DevConfig c, ui
         ss.vol = q.vol;
         ss.seg = 0;
         for (;;) {
-          const Hit sh = trace_closest(s, ss.pos, q.dir, c.eps, errbits);
+          const Hit sh = trace_closest<kCount>(s, ss.pos, q.dir, c.eps, errbits, &tc);
+          if (kCount) {
+            n_trace++;
+            n_hit += sh.slot >= 0 && sh.slot != q.light_slot;
+          }
           if (shadow_segment(s, c, q, sh, p.active, ss)) break;
         }
         if (ss.total > 1e-6f) direct = q.contrib * ss.total;
@@ -101,6 +118,7 @@ __global__ void __launch_bounds__(128) k_render_mega(DevScene s, DevConfig c, ui
         p.plen++;
       } else if (ev.action == 3) {
         p.dir = ev.dir;
+        if (kCount) n_dep += dep != 0.0;
         flush(f, pix, p.active_px, dep);
         dep = 0.0;
         p.active = ev.new_wl;
@@ -114,20 +132,34 @@ __global__ void __launch_bounds__(128) k_render_mega(DevScene s, DevConfig c, ui
       if (++k >= c.max_depth || p.thr == 0.f) done = true;
     }
     if (done) {
+      if (kCount) n_dep += dep != 0.0;
       flush(f, pix, p.active_px, dep);
       pix = -1;
     }
   }
   if (errbits) atomicOr(err, errbits);
+  if (kCount) {
+    atomicAdd(work + 0, (unsigned long long)n_paths);
+    atomicAdd(work + 1, (unsigned long long)n_vert);
+    atomicAdd(work + 2, (unsigned long long)n_trace);
+    atomicAdd(work + 3, (unsigned long long)tc.nodes);
+    atomicAdd(work + 4, (unsigned long long)tc.tris);
+    atomicAdd(work + 5, (unsigned long long)n_hit);
+    atomicAdd(work + 6, (unsigned long long)n_dep);
+  }
 }
 
 }  // namespace
 
 cudaError_t launch_render_mega(const DevScene &s, const DevConfig &c, uint32_t pass, int band, Film f,
-                               int *counter, uint32_t *err, int grid, int block, cudaStream_t st) {
+                               int *counter, uint32_t *err, int grid, int block, cudaStream_t st,
+                               unsigned long long *work) {
   cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), st);
   if (e != cudaSuccess) return e;
-  k_render_mega<<<grid, block, 0, st>>>(s, c, pass, band, f, counter, err);
+  if (work)
+    k_render_mega<true><<<grid, block, 0, st>>>(s, c, pass, band, f, counter, err, work);
+  else
+    k_render_mega<false><<<grid, block, 0, st>>>(s, c, pass, band, f, counter, err, nullptr);
   return cudaGetLastError();
 }
 

@@ -71,7 +71,7 @@ __global__ void k_generate(DevScene s, DevConfig c, uint32_t pass, int band, Wav
 }
 
 // trace(k): shadow chains of shade(k-1), then extension hits of Qk
-__global__ void __launch_bounds__(128) k_trace(DevScene s, DevConfig c, int depth, Film f, WaveBuffers w,
+__global__ void __launch_bounds__(kMaxBlock) k_trace(DevScene s, DevConfig c, int depth, Film f, WaveBuffers w,
                                                uint32_t *__restrict__ err) {
   uint32_t eb = 0;
   const int nsh = depth > 0 ? w.counts[kCntSh + depth - 1] : 0;
@@ -157,7 +157,7 @@ __global__ void k_sort_scatter(DevScene s, DevConfig c, int depth, WaveBuffers w
   }
 }
 
-__global__ void __launch_bounds__(128) k_shade(DevScene s, DevConfig c, uint32_t pass, int band, int depth,
+__global__ void __launch_bounds__(kMaxBlock) k_shade(DevScene s, DevConfig c, uint32_t pass, int band, int depth,
                                                Film f, WaveBuffers w, int use_sorted) {
   const int n = w.counts[kCntExt + depth];
   const int *q = use_sorted ? w.sorted : w.queue[depth & 1];

@@ -60,10 +60,16 @@ TS_D void box_hit(float lox, float hix, float loy, float hiy, float loz, float h
 
 TS_D float cull_bound(float best) { return best + best * (1.0f / 65536.0f); }
 
+// Work counters of one traversal (compiled out unless a kernel asks for them).
+struct TraceCount {
+  uint32_t nodes = 0, tris = 0;
+};
+
 // Fast closest hit.  stack: kStackDepth entries of (node, entry-distance bits)
 // in local memory.  errbits gets kErrStackOverflow if the tree is deeper than
 // the stack (the builder caps depth below it, so this is a guard only).
-TS_D Hit trace_closest(const DevScene &s, float3 o, float3 d, float eps, uint32_t &errbits) {
+template <bool kCount = false>
+TS_D Hit trace_closest(const DevScene &s, float3 o, float3 d, float eps, uint32_t &errbits, TraceCount *tc = nullptr) {
   Hit h;
   h.t = 1e9f;
   h.u = h.v = 0.f;
@@ -77,6 +83,7 @@ TS_D Hit trace_closest(const DevScene &s, float3 o, float3 d, float eps, uint32_
   for (;;) {
     if (node >= 0) {
       const float4 *n = s.node + 4 * (size_t)node;
+      if (kCount) tc->nodes++;
       const float4 a = __ldg(n + 0), b = __ldg(n + 1), c = __ldg(n + 2);
       const int4 l = __ldg(reinterpret_cast<const int4 *>(n) + 3);
       float e0, x0, e1, x1;
@@ -102,6 +109,7 @@ TS_D Hit trace_closest(const DevScene &s, float3 o, float3 d, float eps, uint32_
       const int code = ~node;
       const int first = code >> 4;
       const int cnt = (code & 15) + 1;
+      if (kCount) tc->tris += cnt;
       for (int i = 0; i < cnt; ++i) {
         const float4 *tp = s.tri + 3 * (size_t)(first + i);
         const float4 A = __ldg(tp + 0), E1 = __ldg(tp + 1), E2 = __ldg(tp + 2);

@@ -1,0 +1,44 @@
+"""Multi-GPU sharding of sample passes (one process per GPU).
+
+Paths are independent, so a render shards by sample pass with no exchange in
+the data path: rank r renders its own contiguous run of whole spectral blocks
+(each with its own random streams, since the pass index keys Philox) into its
+own film.  The one exchange is at the end: the FP64 block statistics of all
+ranks are summed (``torch.distributed.all_reduce``, NCCL over NVLink on GPUs,
+gloo on CPUs) into the film of the whole render.
+"""
+import torch
+
+
+def block_range(total_blocks, rank, world):
+    """Contiguous share [first, last) of ``total_blocks`` spectral blocks for ``rank``."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("bad rank/world")
+    base, extra = divmod(int(total_blocks), world)
+    first = rank * base + min(rank, extra)
+    return first, first + base + (1 if rank < extra else 0)
+
+
+def pass_indices(total_blocks, bands, rank, world):
+    """(pass_idx, band) of every pass rank ``rank`` renders, in order."""
+    first, last = block_range(total_blocks, rank, world)
+    return [(b * bands + k, k) for b in range(first, last) for k in range(bands)]
+
+
+def reduce_film(mean, m2, num_blocks, group=None):
+    """Combine per-rank films: mean over all blocks, summed squares, total count.
+
+    mean/m2: float64 tensors of identical shape on every rank; the result
+    replaces them in place on every rank."""
+    import torch.distributed as dist
+    if mean.dtype != torch.float64 or m2.dtype != torch.float64:
+        raise TypeError("film statistics must be float64")
+    n = torch.tensor([float(num_blocks)], dtype=torch.float64, device=mean.device)
+    dist.all_reduce(n, group=group)
+    total = float(n.item())
+    mean.mul_(float(num_blocks))
+    dist.all_reduce(mean, group=group)
+    if total > 0:
+        mean.div_(total)
+    dist.all_reduce(m2, group=group)
+    return mean, m2, int(round(total))

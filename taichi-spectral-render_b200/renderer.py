@@ -185,6 +185,17 @@ class Renderer:
                                             _stream()))
         self.total_samples += 1
 
+    def cast_rays_counted(self, current_sample_in_block, pass_idx=None):
+        """cast_rays through the counting megakernel; returns the work counts."""
+        if pass_idx is None:
+            pass_idx = self.total_samples
+        w = (ctypes.c_uint64 * 8)()
+        self._check(self.lib.ts_render_pass_counted(self._ctx, int(pass_idx) & 0xFFFFFFFF,
+                                                    int(current_sample_in_block), _stream(), w))
+        self.total_samples += 1
+        keys = ("paths", "vertices", "traces", "node_visits", "tri_tests", "hits", "deposits")
+        return {k: int(w[i]) for i, k in enumerate(keys)}
+
     def average_and_reset_block(self, num_blocks_completed):
         """main.py:1592-1607 (FP64 running mean plus the per-cell sum of squares)."""
         self._check(self.lib.ts_accumulate_block(self._ctx, int(num_blocks_completed), _stream()))

@@ -16,7 +16,8 @@ What is pinned (each array is produced by the reference's own code, unmodified):
   not copied: loader tests that need them read the reference tree when it is
   present and are skipped otherwise.
 * ``scene_ref.npz`` -- the reference's default scene (``create_scene``,
-  ``main.py:89-247``) flattened exactly like ``setup_scene`` (``main.py:513-539``),
+  ``main.py:89-247``): its meshes and material dictionaries, and the same
+  scene flattened by ``setup_scene`` (``main.py:513-539``),
   the reference BVH (``build_bvh``, ``main.py:437-507``) with its node table and
   triangle permutation, the scene sizing of ``get_scene_dimensions``
   (``main.py:398-435``) and the per-band light CDF of ``main.py:590-627``.
@@ -150,6 +151,18 @@ def main(ref):
                   mat_eem=g["material_props_single_int"])
         cam = scene["camera"]
         sc["camera"] = np.array([cam["origin"], cam["lookat"], cam["up"]], np.float32)
+        # the scene dictionary itself (inputs of setup_scene), so the package's
+        # flattening can be checked against the reference's
+        import json
+        sc["num_meshes"] = np.int64(len(scene["meshes"]))
+        for mi, mesh in enumerate(scene["meshes"]):
+            sc[f"mesh{mi}_vertices"] = np.asarray(mesh["vertices"], np.float64)
+            sc[f"mesh{mi}_faces"] = np.asarray(mesh["faces"], np.int64)
+            sc[f"mesh{mi}_material_id"] = np.int64(mesh["material_id"])
+            if "vertex_normals" in mesh:
+                sc[f"mesh{mi}_vertex_normals"] = np.asarray(mesh["vertex_normals"], np.float64)
+        to_py = lambda v: [float(x) for x in v] if not isinstance(v, (int, float)) else v
+        sc["materials_json"] = np.array(json.dumps([{k: to_py(v) for k, v in m.items()} for m in mats]))
         np.savez_compressed(os.path.join(here, "scene_ref.npz"), **sc)
         print(f"scene: {T} tris, {N} nodes, {int((ntri > 0).sum())} leaves; dims {dims}")
     finally:

@@ -1,0 +1,65 @@
+"""Pass sharding and the film reduction, on CPU ranks with the gloo backend."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+from helpers import sb  # noqa: F401  (registers the package)
+from spectral_b200 import distributed as sd
+
+
+def test_block_range_partitions():
+    for total in (0, 1, 7, 11, 275 // 25):
+        for world in (1, 2, 3, 8):
+            spans = [sd.block_range(total, r, world) for r in range(world)]
+            assert spans[0][0] == 0 and spans[-1][1] == total
+            assert all(a[1] == b[0] for a, b in zip(spans, spans[1:]))
+            assert max(b - a for a, b in spans) - min(b - a for a, b in spans) <= 1
+    p = sd.pass_indices(4, 25, 1, 2)
+    assert p[0] == (50, 0) and p[-1] == (99, 24) and len(p) == 50
+    with pytest.raises(ValueError):
+        sd.block_range(4, 2, 2)
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _worker(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    rng = np.random.default_rng(rank)
+    nb = 2 + rank  # uneven block counts
+    blocks = rng.uniform(size=(nb, 3, 4, 5))
+    mean = torch.from_numpy(blocks.mean(0).copy())
+    m2 = torch.from_numpy((blocks ** 2).sum(0))
+    mean, m2, total = sd.reduce_film(mean, m2, nb)
+    q.put((rank, mean.numpy(), m2.numpy(), total))
+    dist.destroy_process_group()
+
+
+def test_reduce_film_gloo_world2():
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=120) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    allb = np.concatenate([np.random.default_rng(r).uniform(size=(2 + r, 3, 4, 5)) for r in range(world)])
+    for rank, mean, m2, total in res:
+        assert total == allb.shape[0]
+        assert np.allclose(mean, allb.mean(0), rtol=1e-13)
+        assert np.allclose(m2, (allb ** 2).sum(0), rtol=1e-13)

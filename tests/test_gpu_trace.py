@@ -1,0 +1,113 @@
+"""Closest-hit parity of the CUDA traversal against the oracle (identical rays)."""
+import numpy as np
+import pytest
+import torch
+
+from helpers import camera_rays, golden_compiled, orc, oracle_config, oracle_scene, random_rays, sb
+from spectral_b200 import configs
+
+pytestmark = pytest.mark.gpu
+
+
+def renderer_for(compiled, bvh, cam, **kw):
+    """A Renderer over an already compiled scene (no scene dictionary needed)."""
+    import ctypes
+    cfg = sb.RenderConfig(width=kw.get("width", 16), height=kw.get("height", 16), kernel=kw.get("kernel", "mega"))
+    r = sb.Renderer.__new__(sb.Renderer)
+    r.config, r.lib, r._ctx = cfg, sb.load(), ctypes.c_void_p()
+    sb._lib.check(r.lib.ts_create(ctypes.byref(cfg.to_c()), ctypes.byref(r._ctx)))
+    r.device, r.total_samples, r.num_blocks_completed, r._cam, r.cmf_scale = torch.device("cuda", 0), 0, 0, None, 1.0
+    compiled.bvh = None if bvh is None else {k: np.ascontiguousarray(v) for k, v in bvh.items()}
+    d = compiled.desc()
+    r._check(r.lib.ts_upload_scene(r._ctx, ctypes.byref(d)))
+    r.compiled = compiled
+    r.update_camera(cam["origin"], cam["lookat"], cam["up"])
+    return r
+
+
+def oracle_hits(sc, rays, perm):
+    tri, t, u, v = orc.trace(sc, oracle_config(sb.RenderConfig()), rays)
+    return np.where(tri >= 0, perm[np.maximum(tri, 0)], -1), t, u, v
+
+
+def test_reference_order_is_bit_exact_on_reference_bvh():
+    cs, bvh, cam = golden_compiled()
+    sc = oracle_scene(cs, bvh, cam)
+    rays = np.concatenate([random_rays(100000, 1), camera_rays(cam, 200, 200)], 0)
+    tri_o, t_o, u_o, v_o = oracle_hits(sc, rays, bvh["tri_perm"])
+    with renderer_for(cs, bvh, cam) as r:
+        tri, t, u, v = (x.cpu().numpy() for x in r.trace(torch.from_numpy(rays).cuda(), "reference_order"))
+        assert r.check_device() == 0
+    assert np.array_equal(tri, tri_o)
+    assert np.array_equal(t, t_o) and np.array_equal(u[tri >= 0], u_o[tri >= 0])
+    assert np.array_equal(v[tri >= 0], v_o[tri >= 0])
+
+
+def _near_tie_check(tri, t, tri_o, t_o):
+    mism = tri != tri_o
+    # hit distances: bit-identical on agreeing rays, within 1e-5 relative overall
+    assert np.array_equal(t[~mism], t_o[~mism])
+    hit = tri_o >= 0
+    assert np.all(np.abs(t[hit] - t_o[hit]) <= 1e-5 * t_o[hit])
+    # a differing triangle is only allowed where the two distances tie within 1e-6 t
+    assert np.all(np.abs(t[mism] - t_o[mism]) <= 1e-6 * t_o[mism])
+    return int(mism.sum())
+
+
+def test_fast_traversal_matches_except_near_ties():
+    cs, bvh, cam = golden_compiled()
+    sc = oracle_scene(cs, bvh, cam)
+    rays = np.concatenate([random_rays(100000, 2), camera_rays(cam, 200, 200, jitter_seed=1)], 0)
+    tri_o, t_o, _, _ = oracle_hits(sc, rays, bvh["tri_perm"])
+    with renderer_for(cs, bvh, cam) as r:
+        tri, t, _, _ = (x.cpu().numpy() for x in r.trace(torch.from_numpy(rays).cuda(), "fast"))
+    ties = _near_tie_check(tri, t, tri_o, t_o)
+    assert ties <= 0.002 * len(rays)
+
+
+def test_binned_bvh_traversal_matches_reference_semantics():
+    s, c, ex = configs.box_scene()
+    comp = sb.compile_scene(s, c.bands, eems=ex["eems"], cmf=ex["cmf"])
+    bvh = sb._lib.build_bvh_host(comp.tris["v0"], comp.tris["v1"], comp.tris["v2"])
+    sc = oracle_scene(comp, bvh, s["camera"])
+    rays = np.concatenate([random_rays(100000, 3, lo=-0.49, hi=0.49),
+                           camera_rays(s["camera"], 256, 256, fov_scale=c.fov_scale, jitter_seed=2)], 0)
+    tri_o, t_o, _, _ = oracle_hits(sc, rays, bvh["tri_perm"])
+    # the library builds the same tree itself when none is given
+    with renderer_for(comp, None, s["camera"]) as r:
+        assert np.array_equal(r.tri_perm(), bvh["tri_perm"])
+        for mode in ("fast", "reference_order"):
+            tri, t, _, _ = (x.cpu().numpy() for x in r.trace(torch.from_numpy(rays).cuda(), mode))
+            if mode == "reference_order":
+                assert np.array_equal(tri, tri_o) and np.array_equal(t, t_o)
+            else:
+                assert _near_tie_check(tri, t, tri_o, t_o) <= 0.002 * len(rays)
+
+
+def test_misses_and_degenerate_rays():
+    cs, bvh, cam = golden_compiled()
+    sc = oracle_scene(cs, bvh, cam)
+    # outward rays from outside the box, axis-parallel rays, rays starting on a wall
+    rays = np.array([[0, 0, 5, 0, 0, 1], [0, 0, 5, 0, 0, -1], [0, 0, 0, 1, 0, 0], [0, 0, 0, 0, -1, 0],
+                     [0, -1, 0, 0, 1, 0], [0.3, 0.99, 0.3, 0, -1, 0], [2, 2, 2, 1, 1, 1]], np.float32)
+    rays[:, 3:] /= np.linalg.norm(rays[:, 3:], axis=1, keepdims=True)
+    tri_o, t_o, _, _ = oracle_hits(sc, rays, bvh["tri_perm"])
+    with renderer_for(cs, bvh, cam) as r:
+        for mode in ("fast", "reference_order"):
+            tri, t, _, _ = (x.cpu().numpy() for x in r.trace(torch.from_numpy(rays).cuda(), mode))
+            assert np.array_equal(tri, tri_o) and np.array_equal(t, t_o), mode
+    assert tri_o[0] == -1 and t_o[0] == np.float32(1e9)
+
+
+def test_large_mesh_traversal_matches_oracle():
+    s, c, ex = configs.terrain_scene(grid=256, sphere_slices=100, sphere_stacks=101)
+    comp = sb.compile_scene(s, c.bands, eems=ex["eems"], cmf=ex["cmf"])
+    bvh = sb._lib.build_bvh_host(comp.tris["v0"], comp.tris["v1"], comp.tris["v2"])
+    sc = oracle_scene(comp, bvh, s["camera"])
+    rays = camera_rays(s["camera"], 256, 256, fov_scale=c.fov_scale, jitter_seed=3)
+    tri_o, t_o, _, _ = oracle_hits(sc, rays, bvh["tri_perm"])
+    with renderer_for(comp, bvh, s["camera"]) as r:
+        tri, t, _, _ = (x.cpu().numpy() for x in r.trace(torch.from_numpy(rays).cuda(), "fast"))
+        assert r.check_device() == 0
+    assert _near_tie_check(tri, t, tri_o, t_o) <= 0.002 * len(rays)
+    assert (tri_o >= 0).mean() > 0.3

@@ -1,0 +1,65 @@
+"""The C-ABI library loads and exports every entry point include/spectral.h declares."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from helpers import ROOT, sb
+from spectral_b200 import _lib
+
+
+def declared_functions():
+    src = open(os.path.join(ROOT, "include", "spectral.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(ts_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_header_declares_the_api():
+    names = declared_functions()
+    for must in ("ts_create", "ts_upload_scene", "ts_render_pass", "ts_accumulate_block", "ts_resolve_xyz",
+                 "ts_reset", "ts_trace_batch", "ts_set_camera", "ts_last_error"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.load()
+    bound = {n for n, _, _ in _lib.SIGNATURES}
+    for name in declared_functions():
+        assert hasattr(lib, name), name
+        assert name in bound, f"{name} has no ctypes signature"
+
+
+def test_library_built_for_sm100a():
+    assert os.path.exists(_lib.LIB_PATH)
+    assert b"sm_100a" in _lib.load().ts_version()
+
+
+def test_create_reports_missing_device_cleanly():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    cfg = sb.RenderConfig(width=4, height=4).to_c()
+    ctx = ctypes.c_void_p()
+    st = _lib.load().ts_create(ctypes.byref(cfg), ctypes.byref(ctx))
+    assert st == 2 and not ctx.value
+    assert b"no CUDA device" in _lib.load().ts_last_error(None)
+
+
+def test_config_validation_on_host():
+    lib = _lib.load()
+    ctx = ctypes.c_void_p()
+    for bad in (dict(width=0), dict(bands=0), dict(bands=65), dict(scatter_bounces=0), dict(max_path_length=-1),
+                dict(lambda_min=800.0, lambda_max=400.0)):
+        cfg = sb.RenderConfig(**{**dict(width=4, height=4), **bad}).to_c()
+        assert lib.ts_create(ctypes.byref(cfg), ctypes.byref(ctx)) == 1, bad
+
+
+def test_renderer_refuses_to_run_without_gpu():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from spectral_b200 import configs
+    s, c, ex = configs.box_scene(width=8, height=8)
+    with pytest.raises(RuntimeError, match="no CPU fallback"):
+        sb.Renderer(s, c, eems=ex["eems"], cmf=ex["cmf"])
