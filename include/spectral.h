@@ -128,6 +128,23 @@ ts_status ts_render_pass(ts_ctx *ctx, uint32_t pass_idx, int32_t band, void *str
  * stream is synchronised. */
 ts_status ts_render_pass_counted(ts_ctx *ctx, uint32_t pass_idx, int32_t band, void *stream, uint64_t work[8]);
 
+/* Allocation-free render of one tile (no counterpart in the reference, whose
+ * Taichi runtime allocates everything up front).  For callers that cannot
+ * call cudaMalloc while they render -- an application whose device-memory
+ * budget is fixed after start-up, or a render loop inside another framework
+ * that owns the allocator -- where ts_render_pass's wavefront kernel would
+ * allocate its path-state buffers on first use.  Renders pass pass_idx / band
+ * for the pixels [x0, x0+tile_w) x [y0, y0+tile_h) of the context's scene and
+ * camera, with the same random streams as ts_render_pass, ADDING deposits into
+ * film_dev: a caller-owned [B][H][W] float64 device buffer of the frame.
+ * At most 65536 pixels per call (TS_ERR_CAPACITY beyond).  Its scratch is a
+ * static device array of about 8.4 MB that every GPU loading the library keeps
+ * until exit; the first call on a device looks its address up, so make that
+ * first call before any stream capture.  All calls share the array: calls that
+ * overlap on the GPU race and must be serialised by the caller. */
+ts_status ts_render_tile_noalloc(ts_ctx *ctx, uint32_t pass_idx, int32_t band, int32_t x0, int32_t y0,
+                                 int32_t tile_w, int32_t tile_h, double *film_dev, void *stream);
+
 /* ---- film (average_and_reset_block, clear_pixel_space, main.py:1592-1607, 1661-1674) */
 ts_status ts_accumulate_block(ts_ctx *ctx, int32_t num_blocks_completed, void *stream);
 ts_status ts_reset(ts_ctx *ctx, void *stream);

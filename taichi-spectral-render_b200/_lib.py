@@ -74,6 +74,8 @@ SIGNATURES = [
     ("ts_render_pass", ctypes.c_int, [_VP, ctypes.c_uint32, ctypes.c_int32, _VP]),
     ("ts_render_pass_counted", ctypes.c_int, [_VP, ctypes.c_uint32, ctypes.c_int32, _VP,
                                               ctypes.POINTER(ctypes.c_uint64)]),
+    ("ts_render_tile_noalloc", ctypes.c_int, [_VP, ctypes.c_uint32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                              ctypes.c_int32, ctypes.c_int32, _VP, _VP]),
     ("ts_accumulate_block", ctypes.c_int, [_VP, ctypes.c_int32, _VP]),
     ("ts_reset", ctypes.c_int, [_VP, _VP]),
     ("ts_film_buffer", ctypes.c_int, [_VP, ctypes.c_int32, ctypes.POINTER(F64P), ctypes.POINTER(ctypes.c_size_t)]),

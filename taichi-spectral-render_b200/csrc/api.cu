@@ -479,6 +479,37 @@ ts_status ts_render_pass_counted(ts_ctx *c, uint32_t pass_idx, int32_t band, voi
   return TS_OK;
 }
 
+ts_status ts_render_tile_noalloc(ts_ctx *c, uint32_t pass_idx, int32_t band, int32_t x0, int32_t y0, int32_t tile_w,
+                                 int32_t tile_h, double *film_dev, void *stream) {
+  if (!c || !film_dev) return fail(c, TS_ERR_INVALID_ARG, "ts_render_tile_noalloc: null argument");
+  if (!c->has_scene) return fail(c, TS_ERR_NO_SCENE, "ts_render_tile_noalloc: no scene uploaded");
+  if (band < 0 || band >= c->cfg.bands) return fail(c, TS_ERR_INVALID_ARG, "ts_render_tile_noalloc: band out of range");
+  if (tile_w <= 0 || tile_h <= 0 || x0 < 0 || y0 < 0 || x0 > c->cfg.width - tile_w || y0 > c->cfg.height - tile_h)
+    return fail(c, TS_ERR_INVALID_ARG, "ts_render_tile_noalloc: tile outside the frame");
+  const int64_t n = (int64_t)tile_w * tile_h;
+  if (n > ts::noalloc_max_paths())
+    return fail(c, TS_ERR_CAPACITY, "ts_render_tile_noalloc: a tile of " + std::to_string(n) +
+                                        " pixels exceeds the allocation-free limit of " +
+                                        std::to_string(ts::noalloc_max_paths()) + " pixels per call");
+  TS_CUDA(c, cudaSetDevice(c->cfg.device), "ts_render_tile_noalloc");
+  void *scratch = nullptr;
+  TS_CUDA(c, ts::noalloc_setup(c->cfg.device, &scratch), "ts_render_tile_noalloc: scratch address lookup");
+  ts::Film f;
+  f.block = film_dev;
+  f.mean = nullptr;
+  f.m2 = nullptr;
+  f.W = c->cfg.width;
+  f.H = c->cfg.height;
+  f.B = c->cfg.bands;
+  const int bs = c->cfg.block_size;
+  int per_sm = c->cfg.blocks_per_sm;
+  if (per_sm <= 0) per_sm = std::max(1, 2048 / bs);
+  TS_CUDA(c, ts::launch_wave_tile_noalloc(c->ds, c->dc, pass_idx, band, f, scratch, x0, y0, tile_w, tile_h, c->d_err,
+                                          c->num_sms * per_sm, bs, as_stream(stream)),
+          "ts_render_tile_noalloc");
+  return TS_OK;
+}
+
 ts_status ts_accumulate_block(ts_ctx *c, int32_t n, void *stream) {
   if (!c) return fail(nullptr, TS_ERR_INVALID_ARG, "ts_accumulate_block: null context");
   if (n < 1) return fail(c, TS_ERR_INVALID_ARG, "ts_accumulate_block: num_blocks_completed must be >= 1");

@@ -17,6 +17,8 @@
 // atomics.  With sort_keys set, the shading queue is reordered by the hit
 // material (a counting sort on the device) so that warps shade one material
 // at a time.
+#include <mutex>
+
 #include "estimator.cuh"
 #include "kernels.cuh"
 
@@ -270,6 +272,111 @@ cudaError_t launch_wave_pass(const DevScene &s, const DevConfig &c, uint32_t pas
     k_shade<<<grid, block, 0, st>>>(s, c, pass, band, d, f, w, nkeys ? 1 : 0);
   }
   // the last depth's shadow queries
+  if (c.max_depth > 0) k_trace<<<grid, block, 0, st>>>(s, c, c.max_depth, f, w, err);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free tile pass.
+//
+// Some callers cannot call cudaMalloc when they render: a host application
+// whose device-memory budget is fixed once it has started, or a render loop
+// running inside another framework's callbacks where that framework owns the
+// allocator.  The regular wavefront pass allocates its path-state buffers on
+// first use; this variant takes the same buffers from one fixed, file-scope
+// device array instead, so a call allocates nothing.  The price is a bound on
+// the work of one call: at most kNoAllocMaxPaths pixels (a tile of the frame).
+//
+// Every GPU that loads the library holds the array (about 8.4 MB) until the
+// process exits.  All calls share it: a call clears the counters it needs and
+// overwrites the path state it uses, but two calls whose work overlaps on the
+// GPU (different streams, or different host threads on one device) race on
+// it and must be serialised by the caller.
+namespace {
+
+constexpr int kNoAllocMaxPaths = 65536;
+constexpr size_t kNaVec = (size_t)kNoAllocMaxPaths * 16;  // one float4/int4 per path
+constexpr size_t kNaIdx = (size_t)kNoAllocMaxPaths * 4;   // one int per path
+constexpr size_t kNaCounts = 8192 * sizeof(int);
+constexpr size_t kNaHist = 2 * kMaxKeys * sizeof(int);
+constexpr size_t kNoAllocScratchBytes = 7 * kNaVec + 4 * kNaIdx + kNaCounts + kNaHist;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+// camera rays for the pixels of one tile; path slot s <-> pixel
+// (x0 + s % tw, y0 + s / tw) of the full frame (pixel ids key the random streams)
+__global__ void k_generate_tile(DevScene s, DevConfig c, uint32_t pass, int band, WaveBuffers w, int x0, int y0,
+                                int tw, int th) {
+  const int n = tw * th;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    const int i = x0 + p % tw, j = y0 + p / tw;
+    const int pixel = j * c.W + i;
+    Rng rng;
+    rng.init(c.seed, pass, (uint32_t)pixel, c.scene_id);
+    PathState ps;
+    camera_ray(s, c, i, j, rng, ps, band);
+    w.pos_thr[p] = make_float4(ps.pos.x, ps.pos.y, ps.pos.z, ps.thr);
+    w.dir_spdf[p] = make_float4(ps.dir.x, ps.dir.y, ps.dir.z, ps.spdf);
+    w.meta[p] = make_int4(pixel, band | (band << 8), 0, (int)rng.n);
+    w.queue[0][p] = p;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) w.counts[kCntExt + 0] = n;
+}
+
+// device address of the scratch array, looked up once per device
+std::mutex g_noalloc_mutex;
+void *g_noalloc_ptr[64] = {};
+
+}  // namespace
+
+int noalloc_max_paths() { return kNoAllocMaxPaths; }
+size_t noalloc_scratch_bytes() { return kNoAllocScratchBytes; }
+
+cudaError_t noalloc_setup(int device, void **ptr) {
+  if (device < 0 || device >= 64) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[device]) {
+    // the host-side name of the array is only a stand-in; the kernels need
+    // the address the device uses, looked up with the device current
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    g_noalloc_ptr[device] = p;
+  }
+  *ptr = g_noalloc_ptr[device];
+  return cudaSuccess;
+}
+
+cudaError_t launch_wave_tile_noalloc(const DevScene &s, const DevConfig &c, uint32_t pass, int band, Film f,
+                                     void *scratch, int x0, int y0, int tw, int th, uint32_t *err, int grid,
+                                     int block, cudaStream_t st) {
+  if (c.max_depth > kMaxDepth) return cudaErrorInvalidValue;
+  unsigned char *b = static_cast<unsigned char *>(scratch);
+  WaveBuffers w{};
+  w.pos_thr = reinterpret_cast<float4 *>(b + 0 * kNaVec);
+  w.dir_spdf = reinterpret_cast<float4 *>(b + 1 * kNaVec);
+  w.meta = reinterpret_cast<int4 *>(b + 2 * kNaVec);
+  w.hit = reinterpret_cast<float4 *>(b + 3 * kNaVec);
+  w.sq_origin = reinterpret_cast<float4 *>(b + 4 * kNaVec);
+  w.sq_dir = reinterpret_cast<float4 *>(b + 5 * kNaVec);
+  w.sq_meta = reinterpret_cast<int4 *>(b + 6 * kNaVec);
+  unsigned char *idx = b + 7 * kNaVec;
+  w.queue[0] = reinterpret_cast<int *>(idx + 0 * kNaIdx);
+  w.queue[1] = reinterpret_cast<int *>(idx + 1 * kNaIdx);
+  w.shadow_queue = reinterpret_cast<int *>(idx + 2 * kNaIdx);
+  w.sorted = reinterpret_cast<int *>(idx + 3 * kNaIdx);
+  w.counts = reinterpret_cast<int *>(idx + 4 * kNaIdx);
+  w.key_hist = reinterpret_cast<int *>(idx + 4 * kNaIdx + kNaCounts);
+  w.capacity = kNoAllocMaxPaths;
+  // the array keeps the previous call's contents: the counters must start at zero
+  cudaError_t e = cudaMemsetAsync(w.counts, 0, kNaCounts, st);
+  if (e != cudaSuccess) return e;
+  const int n = tw * th;
+  k_generate_tile<<<(n + 255) / 256, 256, 0, st>>>(s, c, pass, band, w, x0, y0, tw, th);
+  for (int d = 0; d < c.max_depth; ++d) {
+    k_trace<<<grid, block, 0, st>>>(s, c, d, f, w, err);
+    k_shade<<<grid, block, 0, st>>>(s, c, pass, band, d, f, w, 0);
+  }
   if (c.max_depth > 0) k_trace<<<grid, block, 0, st>>>(s, c, c.max_depth, f, w, err);
   return cudaGetLastError();
 }
