@@ -41,6 +41,9 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--kernel", default="mega", choices=["mega", "wavefront"])
     p.add_argument("--workload", default="terrain", choices=["terrain", "box", "volume"])
+    p.add_argument("--width", type=int, default=2, choices=[2, 4, 8], help="BVH node width")
+    p.add_argument("--traversal", default="default", choices=["default", "speculative"])
+    p.add_argument("--budget", type=int, default=0, help="wavefront traversal steps between refills")
     p.add_argument("--no-cpu-baseline", action="store_true")
     return p.parse_args()
 
@@ -226,10 +229,12 @@ def bench_ours(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
     scene, cfg, ex, desc = workload(args.workload)
     cfg.kernel = args.kernel
+    cfg.traversal = args.traversal
+    cfg.trace_budget = args.budget
     cfg.device = local
     comp = sb.compile_scene(scene, cfg.bands, eems=ex["eems"], cmf=ex["cmf"])
     bvh = sb._lib.build_bvh_host(comp.tris["v0"], comp.tris["v1"], comp.tris["v2"])
-    r = sb.Renderer(scene, cfg, eems=ex["eems"], cmf=ex["cmf"], bvh=bvh)
+    r = sb.Renderer(scene, cfg, eems=ex["eems"], cmf=ex["cmf"], bvh=bvh, bvh_params={"width": args.width})
     B = cfg.bands
     paths_per_step = cfg.width * cfg.height
     base_pass = rank * (args.warmup + args.steps + 8) * 4  # disjoint random streams per rank
@@ -296,7 +301,8 @@ def bench_ours(args):
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded procedural scene; no dataset)",
-            "config": {"workload": desc, "kernel": args.kernel, "paths_per_step": paths_per_step,
+            "config": {"workload": desc, "kernel": args.kernel, "bvh_width": args.width, "traversal": args.traversal,
+                       "paths_per_step": paths_per_step,
                        "spp": ex["spp"], "passes_for_spp": cfg.samples_per_pixel,
                        "l2": "inputs larger than L2: scene %.0f MB + film %.0f MB > 126 MB L2; no flush"
                              % ((r.scene_info()["device_bytes"] - 3 * paths_per_step * B * 8) / 1e6,

@@ -34,6 +34,8 @@ typedef enum {
 
 /* Render kernels */
 enum { TS_KERNEL_MEGA = 0, TS_KERNEL_WAVEFRONT = 1 };
+/* Traversal loop of the two-child BVH layout (ts_config.traversal) */
+enum { TS_TRAVERSAL_DEFAULT = 0, TS_TRAVERSAL_SPECULATIVE = 1 };
 /* Traversal modes of ts_trace_batch */
 enum { TS_TRACE_FAST = 0, TS_TRACE_REFERENCE_ORDER = 1 };
 /* Film buffers */
@@ -56,6 +58,8 @@ typedef struct {
   int32_t block_size;            /* threads per block of the render kernels, 32..256 (0 = 128) */
   int32_t blocks_per_sm;         /* persistent grid = SMs * blocks_per_sm (0 = default) */
   int32_t sort_keys;             /* wavefront: sort shading queue by material (0 = off) */
+  int32_t trace_budget;          /* wavefront: traversal steps between refills of idle lanes (0 = 32) */
+  int32_t traversal;             /* TS_TRAVERSAL_DEFAULT or TS_TRAVERSAL_SPECULATIVE (two-child nodes) */
 } ts_config;
 
 /* Scene in the reference's data model (setup_scene, main.py:509-631). Triangles
@@ -83,6 +87,7 @@ typedef struct {
   /* binned-SAH parameters (0 = defaults) */
   int32_t bvh_bins, bvh_leaf_max;
   float bvh_cost_trav, bvh_cost_tri;
+  int32_t bvh_width;                /* device node width 2, 4 or 8 (0 = library default) */
 } ts_scene_desc;
 
 typedef struct {
@@ -90,6 +95,7 @@ typedef struct {
   double sah_cost;
   int32_t max_lights;
   size_t device_bytes;  /* device memory held by the context */
+  int32_t node_width;   /* node width of the uploaded device BVH */
 } ts_scene_info;
 
 /* ---- context (replaces ti.init + the module-global fields, main.py:9, 361-394) */

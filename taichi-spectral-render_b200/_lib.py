@@ -35,7 +35,8 @@ class TsConfig(ctypes.Structure):
                 ("epsilon", ctypes.c_float), ("escape", ctypes.c_float), ("aspect_ratio", ctypes.c_float),
                 ("fov_scale", ctypes.c_float), ("seed", ctypes.c_uint32), ("scene_id", ctypes.c_uint32),
                 ("device", ctypes.c_int32), ("kernel", ctypes.c_int32), ("block_size", ctypes.c_int32),
-                ("blocks_per_sm", ctypes.c_int32), ("sort_keys", ctypes.c_int32)]
+                ("blocks_per_sm", ctypes.c_int32), ("sort_keys", ctypes.c_int32), ("trace_budget", ctypes.c_int32),
+                ("traversal", ctypes.c_int32)]
 
 
 class TsSceneDesc(ctypes.Structure):
@@ -48,13 +49,13 @@ class TsSceneDesc(ctypes.Structure):
                 ("node_left", I32P), ("node_right", I32P), ("node_num_tris", I32P), ("node_tri_start", I32P),
                 ("tri_perm", I32P),
                 ("bvh_bins", ctypes.c_int32), ("bvh_leaf_max", ctypes.c_int32),
-                ("bvh_cost_trav", ctypes.c_float), ("bvh_cost_tri", ctypes.c_float)]
+                ("bvh_cost_trav", ctypes.c_float), ("bvh_cost_tri", ctypes.c_float), ("bvh_width", ctypes.c_int32)]
 
 
 class TsSceneInfo(ctypes.Structure):
     _fields_ = [("num_tris", ctypes.c_int32), ("num_nodes", ctypes.c_int32), ("num_ref_nodes", ctypes.c_int32),
                 ("max_depth", ctypes.c_int32), ("leaves", ctypes.c_int32), ("sah_cost", ctypes.c_double),
-                ("max_lights", ctypes.c_int32), ("device_bytes", ctypes.c_size_t)]
+                ("max_lights", ctypes.c_int32), ("device_bytes", ctypes.c_size_t), ("node_width", ctypes.c_int32)]
 
 
 # (name, restype, argtypes) of every entry point declared in include/spectral.h

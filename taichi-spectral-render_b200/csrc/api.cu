@@ -18,6 +18,7 @@ namespace {
 thread_local std::string g_last_error;
 
 constexpr int kMaxBands = 64;
+constexpr int kDefaultWidth = 2;  // BVH node width when the scene description leaves it at 0
 
 }  // namespace
 
@@ -127,6 +128,8 @@ ts_status ts_create(const ts_config *cfg, ts_ctx **out) {
     return fail(nullptr, TS_ERR_INVALID_ARG, "ts_create: lambda_max_nm must exceed lambda_min_nm");
   if (k.kernel != TS_KERNEL_MEGA && k.kernel != TS_KERNEL_WAVEFRONT)
     return fail(nullptr, TS_ERR_INVALID_ARG, "ts_create: unknown kernel");
+  if (k.traversal != TS_TRAVERSAL_DEFAULT && k.traversal != TS_TRAVERSAL_SPECULATIVE)
+    return fail(nullptr, TS_ERR_INVALID_ARG, "ts_create: unknown traversal variant");
   int ndev = 0;
   cudaError_t e = cudaGetDeviceCount(&ndev);
   if (e != cudaSuccess || ndev == 0) return fail(nullptr, TS_ERR_CUDA, "ts_create: no CUDA device");
@@ -136,6 +139,7 @@ ts_status ts_create(const ts_config *cfg, ts_ctx **out) {
   ts_ctx *c = new ts_ctx();
   c->cfg = k;
   if (c->cfg.block_size <= 0) c->cfg.block_size = 128;
+  if (c->cfg.trace_budget <= 0) c->cfg.trace_budget = 32;
   c->cfg.block_size = std::min(ts::kMaxBlock, std::max(32, c->cfg.block_size / 32 * 32));
   cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, k.device);
   ts::DevConfig &d = c->dc;
@@ -153,6 +157,7 @@ ts_status ts_create(const ts_config *cfg, ts_ctx **out) {
   d.fov = k.fov_scale;
   d.seed = k.seed;
   d.scene_id = k.scene_id;
+  d.speculative = k.traversal == TS_TRAVERSAL_SPECULATIVE ? 1 : 0;
   const size_t cells = (size_t)k.width * k.height * k.bands;
   for (int i = 0; i < 3; ++i) {
     e = cudaMalloc((void **)&c->d_film[i], cells * sizeof(double));
@@ -217,6 +222,8 @@ ts_status ts_upload_scene(ts_ctx *c, const ts_scene_desc *sd) {
   }
 
   // ---- BVH
+  if (sd->bvh_width != 0 && sd->bvh_width != 2 && sd->bvh_width != 4 && sd->bvh_width != 8)
+    return fail(c, TS_ERR_INVALID_ARG, "ts_upload_scene: bvh_width must be 0, 2, 4 or 8");
   ts::BvhOut bvh;
   std::string err;
   if (sd->bvh_num_nodes > 0) {
@@ -225,7 +232,7 @@ ts_status ts_upload_scene(ts_ctx *c, const ts_scene_desc *sd) {
       return fail(c, TS_ERR_INVALID_ARG, "ts_upload_scene: incomplete reference BVH");
     if (!ts::bvh_from_reference(T, sd->v0, sd->v1, sd->v2, sd->bvh_num_nodes, sd->node_min, sd->node_max,
                                 sd->node_left, sd->node_right, sd->node_num_tris, sd->node_tri_start, sd->tri_perm,
-                                bvh, err))
+                                bvh, err, sd->bvh_width > 0 ? sd->bvh_width : kDefaultWidth))
       return fail(c, TS_ERR_INVALID_ARG, "ts_upload_scene: " + err);
   } else {
     ts::BvhParams p;
@@ -233,6 +240,7 @@ ts_status ts_upload_scene(ts_ctx *c, const ts_scene_desc *sd) {
     if (sd->bvh_leaf_max > 0) p.leaf_max = std::min(sd->bvh_leaf_max, ts::kLeafMax);
     if (sd->bvh_cost_trav > 0) p.cost_trav = sd->bvh_cost_trav;
     if (sd->bvh_cost_tri > 0) p.cost_tri = sd->bvh_cost_tri;
+    p.width = sd->bvh_width > 0 ? sd->bvh_width : kDefaultWidth;
     if (!ts::build_bvh_binned(T, sd->v0, sd->v1, sd->v2, p, bvh, err))
       return fail(c, TS_ERR_INVALID_ARG, "ts_upload_scene: " + err);
   }
@@ -342,7 +350,8 @@ ts_status ts_upload_scene(ts_ctx *c, const ts_scene_desc *sd) {
   ds.node = d_node;
   ds.tri = d_tri;
   ds.shade = d_shade;
-  ds.num_nodes = (int)(bvh.node2.size() / 4);
+  ds.node_width = bvh.width;
+  ds.num_nodes = (int)(bvh.node2.size() / ts::node_float4s(bvh.width));
   ds.num_tris = T;
   ds.ref_min = d_rmin;
   ds.ref_max = d_rmax;
@@ -370,6 +379,7 @@ ts_status ts_upload_scene(ts_ctx *c, const ts_scene_desc *sd) {
   c->info.leaves = bvh.leaves;
   c->info.sah_cost = bvh.sah_cost;
   c->info.max_lights = L;
+  c->info.node_width = bvh.width;
   c->has_scene = true;
   // keep the current camera basis
   return ts_set_camera(c, c->cam, c->cam + 3, c->cam + 6);
@@ -454,7 +464,7 @@ ts_status ts_render_pass(ts_ctx *c, uint32_t pass_idx, int32_t band, void *strea
     if (per_sm <= 0) per_sm = std::max(1, 2048 / bs);
     const int grid = c->num_sms * per_sm;
     TS_CUDA(c, ts::launch_wave_pass(c->ds, c->dc, pass_idx, band, film_of(c), c->wave, c->d_err, grid, bs,
-                                    c->cfg.sort_keys, st),
+                                    c->cfg.sort_keys, st, c->cfg.trace_budget),
             "render pass");
   }
   return TS_OK;
@@ -505,7 +515,7 @@ ts_status ts_render_tile_noalloc(ts_ctx *c, uint32_t pass_idx, int32_t band, int
   int per_sm = c->cfg.blocks_per_sm;
   if (per_sm <= 0) per_sm = std::max(1, 2048 / bs);
   TS_CUDA(c, ts::launch_wave_tile_noalloc(c->ds, c->dc, pass_idx, band, f, scratch, x0, y0, tile_w, tile_h, c->d_err,
-                                          c->num_sms * per_sm, bs, as_stream(stream)),
+                                          c->num_sms * per_sm, bs, as_stream(stream), c->cfg.trace_budget),
           "ts_render_tile_noalloc");
   return TS_OK;
 }

@@ -210,11 +210,8 @@ struct Builder {
 
 inline int32_t leaf_code(int first, int count) { return ~((first << 4) | (count - 1)); }
 
-// Flatten a preorder BNode tree into the two-child layout.  Leaves larger than
-// kLeafMax are split into index chunks.  Returns false on a malformed tree.
-bool flatten_two_child(std::vector<BNode> tree, const std::vector<Prim> &prims, const std::vector<int32_t> &perm,
-                       BvhOut &out, std::string &err) {
-  // expand oversized leaves
+// Split leaves larger than kLeafMax into index chunks (new nodes appended).
+void expand_big_leaves(std::vector<BNode> &tree, const std::vector<Prim> &prims, const std::vector<int32_t> &perm) {
   for (size_t i = 0; i < tree.size(); ++i) {
     BNode nd = tree[i];
     if (nd.left < 0 && nd.count > kLeafMax) {
@@ -239,6 +236,105 @@ bool flatten_two_child(std::vector<BNode> tree, const std::vector<Prim> &prims, 
       tree.push_back(c);
     }
   }
+}
+
+// Wide layout: collapse the binary tree greedily (an inner child with the
+// largest surface area is replaced by its two children until a node has
+// `width` children) and store each node's child boxes as SoA float4 rows:
+//   width 4: lo.x hi.x lo.y hi.y lo.z hi.z refs pad         (8 float4, 128 B)
+//   width 8: each of the six rows and the refs as two float4 (16 float4, 256 B)
+// Empty child slots have NaN boxes, which no slab test accepts.  Returns false
+// (out untouched) if the traversal stack bound would be exceeded.
+bool flatten_wide(const std::vector<BNode> &tree, int W, BvhOut &out) {
+  struct WN {
+    int ch[8];
+    int n;
+  };
+  std::vector<WN> wn;
+  std::vector<int> wmap(tree.size(), -1);
+  int max_stack = 0;
+  // iterative DFS over binary inner nodes that start a wide node
+  struct Item {
+    int b, stack_below;
+  };
+  std::vector<Item> todo;
+  const bool root_leaf = tree[0].left < 0;
+  if (root_leaf) {
+    WN w{};
+    w.n = 1;
+    w.ch[0] = 0;
+    wn.push_back(w);
+  } else {
+    todo.push_back({0, 0});
+  }
+  std::vector<std::pair<int, int>> order;  // (binary node, wide index) in creation order
+  while (!todo.empty()) {
+    const Item it = todo.back();
+    todo.pop_back();
+    WN w{};
+    int ch[8] = {tree[it.b].left, tree[it.b].right};
+    int n = 2;
+    while (n < W) {
+      int best = -1;
+      double ba = -1.0;
+      for (int k = 0; k < n; ++k) {
+        if (tree[ch[k]].left < 0) continue;
+        const double a = half_area(tree[ch[k]].lo, tree[ch[k]].hi);
+        if (a > ba) { ba = a; best = k; }
+      }
+      if (best < 0) break;
+      const int b = ch[best];
+      ch[best] = tree[b].left;
+      ch[n++] = tree[b].right;
+    }
+    w.n = n;
+    for (int k = 0; k < n; ++k) w.ch[k] = ch[k];
+    const int me = (int)wn.size();
+    wn.push_back(w);
+    wmap[it.b] = me;
+    const int need = it.stack_below + (n - 1);
+    max_stack = std::max(max_stack, need);
+    for (int k = n - 1; k >= 0; --k)
+      if (tree[ch[k]].left >= 0) todo.push_back({ch[k], need});
+  }
+  if (max_stack > kWideStack) return false;
+  const int F = node_float4s(W);
+  std::vector<float4> nodes((size_t)F * wn.size());
+  const float qnan = std::nanf("");
+  for (size_t i = 0; i < wn.size(); ++i) {
+    float row[6][8];
+    int ref[8];
+    for (int k = 0; k < 8; ++k) {
+      for (int r = 0; r < 6; ++r) row[r][k] = qnan;
+      ref[k] = leaf_code(0, 1);
+    }
+    for (int k = 0; k < wn[i].n; ++k) {
+      const BNode &c = tree[wn[i].ch[k]];
+      row[0][k] = c.lo[0]; row[1][k] = c.hi[0];
+      row[2][k] = c.lo[1]; row[3][k] = c.hi[1];
+      row[4][k] = c.lo[2]; row[5][k] = c.hi[2];
+      ref[k] = c.left >= 0 ? wmap[wn[i].ch[k]] : leaf_code(c.first, c.count);
+    }
+    float4 *dst = nodes.data() + (size_t)F * i;
+    const int per = W / 4;  // float4s per row
+    for (int r = 0; r < 6; ++r)
+      for (int q = 0; q < per; ++q) dst[r * per + q] = make_float4(row[r][4 * q], row[r][4 * q + 1], row[r][4 * q + 2], row[r][4 * q + 3]);
+    for (int q = 0; q < per; ++q) {
+      int4 l = make_int4(ref[4 * q], ref[4 * q + 1], ref[4 * q + 2], ref[4 * q + 3]);
+      std::memcpy(&dst[6 * per + q], &l, sizeof(int4));
+    }
+  }
+  out.node2.swap(nodes);
+  out.width = W;
+  out.stack_need = max_stack;
+  return true;
+}
+
+// Flatten a preorder BNode tree into the device layout (two-child, or wide
+// with `width` 4 or 8).  Returns false on a malformed tree.
+bool flatten_two_child(std::vector<BNode> tree, const std::vector<Prim> &prims, const std::vector<int32_t> &perm,
+                       BvhOut &out, std::string &err, int width = 2) {
+  expand_big_leaves(tree, prims, perm);
   const int N = (int)tree.size();
   if (N == 0) {
     out.node2.clear();
@@ -304,6 +400,9 @@ bool flatten_two_child(std::vector<BNode> tree, const std::vector<Prim> &prims, 
   }
   out.max_depth = maxd;
   out.leaves = leaves;
+  out.width = 2;
+  out.stack_need = maxd;
+  if (width == 4 || width == 8) flatten_wide(tree, width, out);  // keeps the two-child layout if it cannot
   return true;
 }
 
@@ -362,12 +461,12 @@ bool build_bvh_binned(int T, const float *v0, const float *v1, const float *v2, 
     }
   }
   out.sah_cost = cost;
-  return flatten_two_child(std::move(tree), prims, out.perm, out, err);
+  return flatten_two_child(std::move(tree), prims, out.perm, out, err, p.width);
 }
 
 bool bvh_from_reference(int T, const float *v0, const float *v1, const float *v2, int N, const float *nmin,
                         const float *nmax, const int32_t *left, const int32_t *right, const int32_t *ntris,
-                        const int32_t *tstart, const int32_t *perm, BvhOut &out, std::string &err) {
+                        const int32_t *tstart, const int32_t *perm, BvhOut &out, std::string &err, int width) {
   out = BvhOut{};
   if (T < 0 || T >= (1 << 27) || N < 0 || (T > 0 && N == 0)) {
     err = "BVH: bad triangle or node count";
@@ -416,7 +515,7 @@ bool bvh_from_reference(int T, const float *v0, const float *v1, const float *v2
       out.ref_link[i] = make_int4(left[i], right[i], 0, 0);
     }
   }
-  return flatten_two_child(std::move(tree), prims, out.perm, out, err);
+  return flatten_two_child(std::move(tree), prims, out.perm, out, err, width);
 }
 
 }  // namespace ts

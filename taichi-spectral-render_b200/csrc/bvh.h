@@ -15,11 +15,14 @@ struct BvhParams {
   int leaf_max = 8;       // largest leaf the SAH may choose (hard cap 16)
   int sah_depth = 40;     // below this depth, object-median splits only (bounds the tree depth)
   int threads = 0;        // 0 = hardware concurrency
+  int width = 2;          // node width of the device layout: 2, 4 or 8
 };
 
 struct BvhOut {
   std::vector<int32_t> perm;   // slot -> original triangle index
-  std::vector<float4> node2;   // two-child layout, 4 x float4 per node
+  std::vector<float4> node2;   // device layout: width 2 -> 4 float4 per node, 4 -> 8, 8 -> 16
+  int width = 2;               // node width of node2 (a wide layout falls back to 2 if its stack bound is exceeded)
+  int stack_need = 0;          // deepest traversal stack the device layout can require
   std::vector<float> ref_min, ref_max;  // reference layout, [N][3]
   std::vector<int4> ref_link;           // (left, right, num_tris, tri_start)
   int max_depth = 0;
@@ -31,10 +34,14 @@ struct BvhOut {
 bool build_bvh_binned(int T, const float *v0, const float *v1, const float *v2, const BvhParams &p, BvhOut &out,
                       std::string &err);
 
+// Floats per node of the device layout for a node width.
+inline int node_float4s(int width) { return width == 8 ? 16 : (width == 4 ? 8 : 4); }
+
 // Adopt a tree given in the reference layout (e.g. produced by the reference's
 // own build_bvh, main.py:437-507): perm[slot] = original triangle index.
 bool bvh_from_reference(int T, const float *v0, const float *v1, const float *v2, int N, const float *nmin,
                         const float *nmax, const int32_t *left, const int32_t *right, const int32_t *ntris,
-                        const int32_t *tstart, const int32_t *perm, BvhOut &out, std::string &err);
+                        const int32_t *tstart, const int32_t *perm, BvhOut &out, std::string &err,
+                        int width = 2);
 
 }  // namespace ts

@@ -31,6 +31,7 @@ struct DevConfig {
   int32_t max_depth, scatter_bounces;
   float aspect, fov;
   uint32_t seed, scene_id;
+  int32_t speculative;  // two-child layout: speculative while-while traversal
 };
 
 // Device scene.  Triangles are in BVH leaf order ("slot" order).
@@ -38,6 +39,8 @@ struct DevConfig {
 //   tri[3*s+1] = (e1.xyz, material bits)     e1 = v1 - v0 (float32)
 //   tri[3*s+2] = (e2.xyz, 0)                 e2 = v2 - v0 (float32)
 //   shade[3*s+k] = (n_k.xyz, geometric_normal[k])
+// Wide nodes (width 4 / 8): six rows of child-box bounds (lo.x hi.x lo.y hi.y
+// lo.z hi.z, one float per child) followed by the child links, 128 / 256 B.
 // Two-child BVH nodes, 64 B each:
 //   node[4*i+0] = (c0.lo.x, c0.hi.x, c0.lo.y, c0.hi.y)
 //   node[4*i+1] = (c1.lo.x, c1.hi.x, c1.lo.y, c1.hi.y)
@@ -47,10 +50,11 @@ struct DevConfig {
 // Reference-layout nodes (main.py:267-275) are kept for the exact-order
 // traversal used by parity checks.
 struct DevScene {
-  const float4 *__restrict__ node;
+  const float4 *__restrict__ node;    // device BVH layout (node_width children per node)
   const float4 *__restrict__ tri;
   const float4 *__restrict__ shade;
   int32_t num_nodes, num_tris;
+  int32_t node_width;                 // 2, 4 or 8
   const float *__restrict__ ref_min;
   const float *__restrict__ ref_max;
   const int4 *__restrict__ ref_link;  // (left, right, num_tris, tri_start)

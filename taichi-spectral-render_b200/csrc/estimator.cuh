@@ -382,6 +382,19 @@ struct ShadowState {
   float total, traveled;
   int vol, seg;
 };
+
+// Distance bound for the trace of the next shadow segment.  In a medium that
+// neither absorbs nor scatters at this band (air), hits beyond the light do
+// not change the transmittance -- exp(-0 * t) = 1 for any t, and such a hit
+// counts as reaching the light -- so the traversal may stop at the light.  In
+// any other medium the reference attenuates over the distance to the next
+// surface even beyond the light (main.py:1459-1462), which needs the true
+// closest hit.
+TS_D float shadow_bound(const DevScene &s, const DevConfig &c, const ShadowQuery &q, const ShadowState &st,
+                        int band) {
+  const Mat vm = get_mat(s, c.B, st.vol, band);
+  return absorb_m(c, vm.k, band) + vm.sigma_s == 0.f ? q.max_dist - st.traveled : 1e9f;
+}
 TS_D bool shadow_segment(const DevScene &s, const DevConfig &c, const ShadowQuery &q, const Hit &hit, int band,
                          ShadowState &st) {
   const Mat vm = get_mat(s, c.B, st.vol, band);

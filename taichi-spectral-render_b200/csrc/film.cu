@@ -86,6 +86,7 @@ __global__ void k_resolve_rgb(Film f, const float *__restrict__ cmf, double scal
 }
 
 // visualize_normals, main.py:1631-1659 (render-resolution part)
+template <int W>
 __global__ void k_normals(DevScene s, DevConfig c, float *__restrict__ out, uint32_t *err) {
   const int npix = c.W * c.H;
   uint32_t eb = 0;
@@ -95,7 +96,7 @@ __global__ void k_normals(DevScene s, DevConfig c, float *__restrict__ out, uint
     const float v = ((float)j + 0.5f) / (float)c.H;
     const float3 d = normalize(s.cam_u * ((u * 2.0f - 1.0f) * c.aspect * c.fov) +
                                s.cam_v * ((v * 2.0f - 1.0f) * c.fov) - s.cam_w * 2.0f);
-    const Hit h = trace_closest(s, s.cam_o, d, c.eps, eb);
+    const Hit h = trace_closest<W>(s, s.cam_o, d, c.eps, eb);
     float3 col = f3(0.f, 0.f, 0.f);
     if (h.slot >= 0) col = surface_info(s, h, d).ns * 0.5f + f3(0.5f, 0.5f, 0.5f);
     out[3 * (size_t)p + 0] = col.x;
@@ -105,7 +106,7 @@ __global__ void k_normals(DevScene s, DevConfig c, float *__restrict__ out, uint
   if (eb) atomicOr(err, eb);
 }
 
-template <int kMode>
+template <int kMode, int W>
 __global__ void k_trace_batch(DevScene s, float eps, const float *__restrict__ rays, int n,
                               int32_t *__restrict__ tri_orig, float *__restrict__ t, float *__restrict__ u,
                               float *__restrict__ v, uint32_t *err) {
@@ -113,7 +114,7 @@ __global__ void k_trace_batch(DevScene s, float eps, const float *__restrict__ r
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
     const float *q = rays + 6 * (size_t)r;
     const float3 o = f3(q[0], q[1], q[2]), d = f3(q[3], q[4], q[5]);
-    const Hit h = kMode == 0 ? trace_closest(s, o, d, eps, eb) : trace_reference_order(s, o, d, eps, eb);
+    const Hit h = kMode == 0 ? trace_closest<W>(s, o, d, eps, eb) : trace_reference_order(s, o, d, eps, eb);
     tri_orig[r] = h.slot >= 0 ? __float_as_int(__ldg(s.tri + 3 * (size_t)h.slot).w) : -1;
     t[r] = h.t;
     if (u) u[r] = h.u;
@@ -143,16 +144,20 @@ cudaError_t launch_resolve_rgb(Film f, const float *cmf, double scale, const flo
 }
 cudaError_t launch_render_normals(const DevScene &s, const DevConfig &c, float *out, uint32_t *err,
                                   cudaStream_t st) {
-  k_normals<<<grid_for((size_t)c.W * c.H), kThreads, 0, st>>>(s, c, out, err);
+  const int g = grid_for((size_t)c.W * c.H);
+  if (s.node_width == 8) k_normals<8><<<g, kThreads, 0, st>>>(s, c, out, err);
+  else if (s.node_width == 4) k_normals<4><<<g, kThreads, 0, st>>>(s, c, out, err);
+  else k_normals<2><<<g, kThreads, 0, st>>>(s, c, out, err);
   return cudaGetLastError();
 }
 cudaError_t launch_trace_batch(const DevScene &s, float eps, const float *rays, int n, int mode, int32_t *tri_orig,
                                float *t, float *u, float *v, uint32_t *err, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
-  if (mode == 0)
-    k_trace_batch<0><<<grid_for((size_t)n), kThreads, 0, st>>>(s, eps, rays, n, tri_orig, t, u, v, err);
-  else
-    k_trace_batch<1><<<grid_for((size_t)n), kThreads, 0, st>>>(s, eps, rays, n, tri_orig, t, u, v, err);
+  const int g = grid_for((size_t)n);
+  if (mode != 0) k_trace_batch<1, 2><<<g, kThreads, 0, st>>>(s, eps, rays, n, tri_orig, t, u, v, err);
+  else if (s.node_width == 8) k_trace_batch<0, 8><<<g, kThreads, 0, st>>>(s, eps, rays, n, tri_orig, t, u, v, err);
+  else if (s.node_width == 4) k_trace_batch<0, 4><<<g, kThreads, 0, st>>>(s, eps, rays, n, tri_orig, t, u, v, err);
+  else k_trace_batch<0, 2><<<g, kThreads, 0, st>>>(s, eps, rays, n, tri_orig, t, u, v, err);
   return cudaGetLastError();
 }
 

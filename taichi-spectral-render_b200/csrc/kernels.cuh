@@ -56,7 +56,7 @@ constexpr int kMaxKeys = 256;
 
 cudaError_t launch_wave_pass(const DevScene &s, const DevConfig &c, uint32_t pass, int band, Film f,
                              const WaveBuffers &w, uint32_t *err, int grid, int block, int sort_keys,
-                             cudaStream_t st);
+                             cudaStream_t st, int trace_budget);
 
 // Allocation-free tile pass (render_wave.cu): scratch from a static device array.
 int noalloc_max_paths();
@@ -64,6 +64,6 @@ size_t noalloc_scratch_bytes();
 cudaError_t noalloc_setup(int device, void **ptr);
 cudaError_t launch_wave_tile_noalloc(const DevScene &s, const DevConfig &c, uint32_t pass, int band, Film f,
                                      void *scratch, int x0, int y0, int tw, int th, uint32_t *err, int grid,
-                                     int block, cudaStream_t st);
+                                     int block, cudaStream_t st, int trace_budget);
 
 }  // namespace ts

@@ -24,8 +24,8 @@ __device__ __forceinline__ void flush(Film f, int pixel, int band, double dep) {
 // kCount: also count the work (for the roofline's algorithmic bytes):
 // work[0..7] = paths, path vertices, traversals, node visits, triangle tests,
 // surface hits resolved, film deposits, (unused).
-template <bool kCount>
-__global__ void __launch_bounds__(kMaxBlock) k_render_mega(DevScene s, DevConfig c, uint32_t pass, int band, Film f,
+template <int W, bool kCount>
+__global__ void __launch_bounds__(128, 5) k_render_mega(DevScene s, DevConfig c, uint32_t pass, int band, Film f,
                                                      int *__restrict__ counter, uint32_t *__restrict__ err,
                                                      unsigned long long *__restrict__ work) {
   const int lane = threadIdx.x & 31;
@@ -66,7 +66,8 @@ __global__ void __launch_bounds__(kMaxBlock) k_render_mega(DevScene s, DevConfig
 
     // ---- one path vertex (one iteration of the loop at main.py:1534)
     bool done = false;
-    const Hit h = trace_closest<kCount>(s, p.pos, p.dir, c.eps, errbits, &tc);
+    // hits beyond ESCAPE count as escapes (main.py:1209-1214): traverse no further
+    const Hit h = trace_closest<W, kCount>(s, p.pos, p.dir, c.eps, errbits, &tc, c.escape);
     const VolEvent ev = volume_event(s, c, p, h, rng);
     if (kCount) {
       n_trace++;
@@ -100,7 +101,8 @@ __global__ void __launch_bounds__(kMaxBlock) k_render_mega(DevScene s, DevConfig
         ss.vol = q.vol;
         ss.seg = 0;
         for (;;) {
-          const Hit sh = trace_closest<kCount>(s, ss.pos, q.dir, c.eps, errbits, &tc);
+          const Hit sh =
+              trace_closest<W, kCount>(s, ss.pos, q.dir, c.eps, errbits, &tc, shadow_bound(s, c, q, ss, p.active));
           if (kCount) {
             n_trace++;
             n_hit += sh.slot >= 0 && sh.slot != q.light_slot;
@@ -156,10 +158,20 @@ cudaError_t launch_render_mega(const DevScene &s, const DevConfig &c, uint32_t p
                                unsigned long long *work) {
   cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), st);
   if (e != cudaSuccess) return e;
-  if (work)
-    k_render_mega<true><<<grid, block, 0, st>>>(s, c, pass, band, f, counter, err, work);
-  else
-    k_render_mega<false><<<grid, block, 0, st>>>(s, c, pass, band, f, counter, err, nullptr);
+  block = block > 128 ? 128 : block;  // the kernel is compiled for blocks of at most 128 threads
+  if (s.node_width == 8) {
+    if (work) k_render_mega<8, true><<<grid, block, 0, st>>>(s, c, pass, band, f, counter, err, work);
+    else k_render_mega<8, false><<<grid, block, 0, st>>>(s, c, pass, band, f, counter, err, nullptr);
+  } else if (s.node_width == 4) {
+    if (work) k_render_mega<4, true><<<grid, block, 0, st>>>(s, c, pass, band, f, counter, err, work);
+    else k_render_mega<4, false><<<grid, block, 0, st>>>(s, c, pass, band, f, counter, err, nullptr);
+  } else if (c.speculative) {
+    if (work) k_render_mega<3, true><<<grid, block, 0, st>>>(s, c, pass, band, f, counter, err, work);
+    else k_render_mega<3, false><<<grid, block, 0, st>>>(s, c, pass, band, f, counter, err, nullptr);
+  } else {
+    if (work) k_render_mega<2, true><<<grid, block, 0, st>>>(s, c, pass, band, f, counter, err, work);
+    else k_render_mega<2, false><<<grid, block, 0, st>>>(s, c, pass, band, f, counter, err, nullptr);
+  }
   return cudaGetLastError();
 }
 

@@ -72,49 +72,89 @@ __global__ void k_generate(DevScene s, DevConfig c, uint32_t pass, int band, Wav
   if (blockIdx.x == 0 && threadIdx.x == 0) w.counts[kCntExt + 0] = npix;
 }
 
-// trace(k): shadow chains of shade(k-1), then extension hits of Qk
-__global__ void __launch_bounds__(kMaxBlock) k_trace(DevScene s, DevConfig c, int depth, Film f, WaveBuffers w,
-                                               uint32_t *__restrict__ err) {
+// trace(k): shadow chains of shade(k-1), then extension hits of Qk.
+// Persistent lanes with per-lane refill: each lane traverses its current ray
+// for at most `budget` steps; lanes whose ray has finished then take new work
+// items (one atomic per warp), so a warp does not idle behind its longest ray.
+template <int W>
+__global__ void __launch_bounds__(kMaxBlock, 4) k_trace(DevScene s, DevConfig c, int depth, Film f, WaveBuffers w,
+                                                     uint32_t *__restrict__ err, int budget) {
   uint32_t eb = 0;
   const int nsh = depth > 0 ? w.counts[kCntSh + depth - 1] : 0;
   const int next = depth < c.max_depth ? w.counts[kCntExt + depth] : 0;
   const int *q = w.queue[depth & 1];
   const int total = nsh + next;
   int *fetch = w.counts + kCntFetchT + depth;
+  const int lane = threadIdx.x & 31;
+  int item = -1, pid = 0, pixel = 0, band = 0, dep_band = 0;
+  bool exhausted = false;
+  Traversal t;
+  int2 stack[StackSize<W>::value];
+  ShadowQuery sq;
+  ShadowState ss;
   for (;;) {
-    const int base = warp_fetch(fetch);
-    if (base >= total) break;
-    const int i = base + (threadIdx.x & 31);
-    if (i < nsh) {
-      const float4 o = w.sq_origin[i], d = w.sq_dir[i];
-      const int4 m = w.sq_meta[i];
-      ShadowQuery sq;
-      sq.origin = xyz(o);
-      sq.max_dist = o.w;
-      sq.dir = xyz(d);
-      sq.contrib = d.w;
-      sq.light_slot = m.y;
-      sq.vol = m.z;
-      const int band = m.w & 0xff, dep_band = m.w >> 8;
-      ShadowState ss;
-      ss.pos = sq.origin;
-      ss.total = 1.f;
-      ss.traveled = 0.f;
-      ss.vol = sq.vol;
-      ss.seg = 0;
-      for (;;) {
-        const Hit h = trace_closest(s, ss.pos, sq.dir, c.eps, eb);
-        if (shadow_segment(s, c, sq, h, band, ss)) break;
+    const bool need = item < 0 && !exhausted;
+    const unsigned m = __ballot_sync(0xffffffffu, need);
+    if (m) {
+      const int leader = __ffs(m) - 1;
+      int base = 0;
+      if (lane == leader) base = atomicAdd(fetch, __popc(m));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (need) {
+        const int idx = base + __popc(m & ((1u << lane) - 1u));
+        if (idx >= total) {
+          exhausted = true;
+        } else if (idx < nsh) {
+          item = idx;
+          const float4 o = w.sq_origin[idx], d = w.sq_dir[idx];
+          const int4 mm = w.sq_meta[idx];
+          sq.origin = xyz(o);
+          sq.max_dist = o.w;
+          sq.dir = xyz(d);
+          sq.contrib = d.w;
+          sq.light_slot = mm.y;
+          sq.vol = mm.z;
+          pixel = mm.x;
+          band = mm.w & 0xff;
+          dep_band = mm.w >> 8;
+          ss.pos = sq.origin;
+          ss.total = 1.f;
+          ss.traveled = 0.f;
+          ss.vol = sq.vol;
+          ss.seg = 0;
+          trav_begin(s, t, ss.pos, sq.dir, shadow_bound(s, c, sq, ss, band));
+        } else {
+          item = idx;
+          pid = q[idx - nsh];
+          const float4 pt = w.pos_thr[pid], ds = w.dir_spdf[pid];
+          trav_begin(s, t, xyz(pt), xyz(ds), c.escape);
+        }
       }
-      if (ss.total > 1e-6f) deposit(f, m.x, dep_band, sq.contrib * ss.total);
-    } else if (i < total) {
-      const int pid = q[i - nsh];
-      const float4 pt = w.pos_thr[pid], ds = w.dir_spdf[pid];
-      const Hit h = trace_closest(s, xyz(pt), xyz(ds), c.eps, eb);
-      w.hit[pid] = make_float4(h.t, h.u, h.v, __int_as_float(h.slot));
+    }
+    if (__ballot_sync(0xffffffffu, item >= 0) == 0) break;
+    if (item >= 0 && trav_advance<W>(s, t, stack, c.eps, budget, eb)) {
+      if (item < nsh) {
+        if (shadow_segment(s, c, sq, t.h, band, ss)) {
+          if (ss.total > 1e-6f) deposit(f, pixel, dep_band, sq.contrib * ss.total);
+          item = -1;
+        } else {
+          trav_begin(s, t, ss.pos, sq.dir, shadow_bound(s, c, sq, ss, band));
+        }
+      } else {
+        w.hit[pid] = make_float4(t.h.t, t.h.u, t.h.v, __int_as_float(t.h.slot));
+        item = -1;
+      }
     }
   }
   if (eb) atomicOr(err, eb);
+}
+
+void launch_trace(const DevScene &s, const DevConfig &c, int depth, Film f, const WaveBuffers &w, uint32_t *err,
+                  int grid, int block, cudaStream_t st, int budget) {
+  if (s.node_width == 8) k_trace<8><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget);
+  else if (s.node_width == 4) k_trace<4><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget);
+  else if (c.speculative) k_trace<3><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget);
+  else k_trace<2><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget);
 }
 
 // material key of a queued path for the shading sort (num_materials = miss)
@@ -250,7 +290,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_shade(DevScene s, DevConfig c, ui
 
 cudaError_t launch_wave_pass(const DevScene &s, const DevConfig &c, uint32_t pass, int band, Film f,
                              const WaveBuffers &w, uint32_t *err, int grid, int block, int sort_keys,
-                             cudaStream_t st) {
+                             cudaStream_t st, int trace_budget) {
   if (c.max_depth > kMaxDepth) return cudaErrorInvalidValue;
   cudaError_t e = cudaMemsetAsync(w.counts, 0, kCntTotal * sizeof(int), st);
   if (e != cudaSuccess) return e;
@@ -263,7 +303,7 @@ cudaError_t launch_wave_pass(const DevScene &s, const DevConfig &c, uint32_t pas
     if (e != cudaSuccess) return e;
   }
   for (int d = 0; d < c.max_depth; ++d) {
-    k_trace<<<grid, block, 0, st>>>(s, c, d, f, w, err);
+    launch_trace(s, c, d, f, w, err, grid, block, st, trace_budget);
     if (nkeys) {
       k_sort_count<<<grid, 256, 0, st>>>(s, c, d, w, nkeys);
       k_sort_scan<<<1, 32, 0, st>>>(w, nkeys);
@@ -272,7 +312,7 @@ cudaError_t launch_wave_pass(const DevScene &s, const DevConfig &c, uint32_t pas
     k_shade<<<grid, block, 0, st>>>(s, c, pass, band, d, f, w, nkeys ? 1 : 0);
   }
   // the last depth's shadow queries
-  if (c.max_depth > 0) k_trace<<<grid, block, 0, st>>>(s, c, c.max_depth, f, w, err);
+  if (c.max_depth > 0) launch_trace(s, c, c.max_depth, f, w, err, grid, block, st, trace_budget);
   return cudaGetLastError();
 }
 
@@ -349,7 +389,7 @@ cudaError_t noalloc_setup(int device, void **ptr) {
 
 cudaError_t launch_wave_tile_noalloc(const DevScene &s, const DevConfig &c, uint32_t pass, int band, Film f,
                                      void *scratch, int x0, int y0, int tw, int th, uint32_t *err, int grid,
-                                     int block, cudaStream_t st) {
+                                     int block, cudaStream_t st, int trace_budget) {
   if (c.max_depth > kMaxDepth) return cudaErrorInvalidValue;
   unsigned char *b = static_cast<unsigned char *>(scratch);
   WaveBuffers w{};
@@ -374,10 +414,10 @@ cudaError_t launch_wave_tile_noalloc(const DevScene &s, const DevConfig &c, uint
   const int n = tw * th;
   k_generate_tile<<<(n + 255) / 256, 256, 0, st>>>(s, c, pass, band, w, x0, y0, tw, th);
   for (int d = 0; d < c.max_depth; ++d) {
-    k_trace<<<grid, block, 0, st>>>(s, c, d, f, w, err);
+    launch_trace(s, c, d, f, w, err, grid, block, st, trace_budget);
     k_shade<<<grid, block, 0, st>>>(s, c, pass, band, d, f, w, 0);
   }
-  if (c.max_depth > 0) k_trace<<<grid, block, 0, st>>>(s, c, c.max_depth, f, w, err);
+  if (c.max_depth > 0) launch_trace(s, c, c.max_depth, f, w, err, grid, block, st, trace_budget);
   return cudaGetLastError();
 }
 

@@ -19,6 +19,8 @@
 // the reference: explicit 64-entry stack, left pushed before right (so right
 // is popped first), no distance culling.
 #pragma once
+#include <climits>
+
 #include "common.cuh"
 
 namespace ts {
@@ -65,48 +67,67 @@ struct TraceCount {
   uint32_t nodes = 0, tris = 0;
 };
 
-// Fast closest hit.  stack: kStackDepth entries of (node, entry-distance bits)
-// in local memory.  errbits gets kErrStackOverflow if the tree is deeper than
-// the stack (the builder caps depth below it, so this is a guard only).
-template <bool kCount = false>
-TS_D Hit trace_closest(const DevScene &s, float3 o, float3 d, float eps, uint32_t &errbits, TraceCount *tc = nullptr) {
+// Resumable fast traversal.  The state lives in registers; the stack of
+// (node, entry-distance bits) pairs is owned by the caller so that a lane can
+// stop after a budget of steps and resume later (the persistent trace kernel
+// refills idle lanes between budgets).
+constexpr int kTravDone = -2147483647 - 1;  // never a leaf code: first slot < 2^27 - 1
+
+struct Traversal {
+  float3 o, d, inv;
+  float tcull;
   Hit h;
-  h.t = 1e9f;
-  h.u = h.v = 0.f;
-  h.slot = -1;
-  if (s.num_nodes <= 0) return h;
-  const float3 inv = f3(__frcp_rn(d.x), __frcp_rn(d.y), __frcp_rn(d.z));
-  int2 stack[kStackDepth];
-  int sp = 0;
-  int node = 0;
-  float tcull = cull_bound(h.t);
-  for (;;) {
-    if (node >= 0) {
-      const float4 *n = s.node + 4 * (size_t)node;
+  int node, sp;
+};
+
+// bound: distance beyond which hits do not matter to the caller.  Boxes past
+// it are skipped; a hit beyond it may still be returned (callers treat such a
+// hit like a miss), so results are the same as with bound = 1e9.
+TS_D void trav_begin(const DevScene &s, Traversal &t, float3 o, float3 d, float bound) {
+  t.o = o;
+  t.d = d;
+  t.inv = f3(__frcp_rn(d.x), __frcp_rn(d.y), __frcp_rn(d.z));
+  t.h.t = 1e9f;
+  t.h.u = t.h.v = 0.f;
+  t.h.slot = -1;
+  t.tcull = cull_bound(fminf(bound, 1e9f));
+  t.node = s.num_nodes > 0 ? 0 : kTravDone;
+  t.sp = 0;
+}
+
+// Advance by at most `budget` steps (one inner node, or one leaf and the pop
+// that follows).  Returns true once the traversal has finished.
+template <bool kCount = false>
+TS_D bool trav_steps(const DevScene &s, Traversal &t, int2 *stack, float eps, int budget, uint32_t &errbits,
+                     TraceCount *tc = nullptr) {
+  for (int it = 0; it < budget; ++it) {
+    if (t.node == kTravDone) return true;
+    if (t.node >= 0) {
+      const float4 *n = s.node + 4 * (size_t)t.node;
       if (kCount) tc->nodes++;
       const float4 a = __ldg(n + 0), b = __ldg(n + 1), c = __ldg(n + 2);
       const int4 l = __ldg(reinterpret_cast<const int4 *>(n) + 3);
       float e0, x0, e1, x1;
-      box_hit(a.x, a.y, a.z, a.w, c.x, c.y, o, inv, e0, x0);
-      box_hit(b.x, b.y, b.z, b.w, c.z, c.w, o, inv, e1, x1);
-      const bool h0 = e0 < x0 && x0 > 0.f && e0 <= tcull;
-      const bool h1 = e1 < x1 && x1 > 0.f && e1 <= tcull;
+      box_hit(a.x, a.y, a.z, a.w, c.x, c.y, t.o, t.inv, e0, x0);
+      box_hit(b.x, b.y, b.z, b.w, c.z, c.w, t.o, t.inv, e1, x1);
+      const bool h0 = e0 < x0 && x0 > 0.f && e0 <= t.tcull;
+      const bool h1 = e1 < x1 && x1 > 0.f && e1 <= t.tcull;
       if (h0 && h1) {
         int nr = l.x, fr = l.y;
         float fe = e1;
         if (e1 < e0) { nr = l.y; fr = l.x; fe = e0; }
-        if (sp < kStackDepth) {
-          stack[sp++] = make_int2(fr, __float_as_int(fe));
+        if (t.sp < kStackDepth) {
+          stack[t.sp++] = make_int2(fr, __float_as_int(fe));
         } else {
           errbits |= kErrStackOverflow;
         }
-        node = nr;
+        t.node = nr;
         continue;
       }
-      if (h0) { node = l.x; continue; }
-      if (h1) { node = l.y; continue; }
+      if (h0) { t.node = l.x; continue; }
+      if (h1) { t.node = l.y; continue; }
     } else {
-      const int code = ~node;
+      const int code = ~t.node;
       const int first = code >> 4;
       const int cnt = (code & 15) + 1;
       if (kCount) tc->tris += cnt;
@@ -114,23 +135,260 @@ TS_D Hit trace_closest(const DevScene &s, float3 o, float3 d, float eps, uint32_
         const float4 *tp = s.tri + 3 * (size_t)(first + i);
         const float4 A = __ldg(tp + 0), E1 = __ldg(tp + 1), E2 = __ldg(tp + 2);
         float u, v;
-        const float t = tri_hit(o, d, A, E1, E2, eps, u, v);
-        if (t > eps && t < h.t) {
-          h.t = t;
-          h.u = u;
-          h.v = v;
-          h.slot = first + i;
-          tcull = cull_bound(t);
+        const float tt = tri_hit(t.o, t.d, A, E1, E2, eps, u, v);
+        if (tt > eps && tt < t.h.t) {
+          t.h.t = tt;
+          t.h.u = u;
+          t.h.v = v;
+          t.h.slot = first + i;
+          t.tcull = fminf(t.tcull, cull_bound(tt));
         }
       }
     }
-    // pop the next box that is still closer than the best hit
+    // pop the next box that is still closer than the cull bound
     for (;;) {
-      if (sp == 0) return h;
-      const int2 e = stack[--sp];
-      if (__int_as_float(e.y) <= tcull) { node = e.x; break; }
+      if (t.sp == 0) {
+        t.node = kTravDone;
+        return true;
+      }
+      const int2 e = stack[--t.sp];
+      if (__int_as_float(e.y) <= t.tcull) {
+        t.node = e.x;
+        break;
+      }
     }
   }
+  return t.node == kTravDone;
+}
+
+// Speculative while-while traversal of the two-child layout (Aila & Laine,
+// "Understanding the efficiency of ray traversal on GPUs", HPG 2009): a lane
+// that reaches a leaf postpones it and keeps descending, and the warp tests
+// leaves only once every active lane holds one (or has finished), so leaf
+// tests and inner-node steps are not interleaved across the warp.  Same
+// results as trav_steps.
+template <bool kCount = false>
+TS_D bool trav_steps_spec(const DevScene &s, Traversal &t, int2 *stack, float eps, int budget, uint32_t &errbits,
+                          TraceCount *tc = nullptr) {
+  int leaf = 0;  // postponed leaf code (< 0), or 0
+  for (int it = 0; it < budget; ++it) {
+    if (t.node == kTravDone && leaf == 0) return true;
+    // ---- inner nodes
+    while (t.node >= 0) {
+      const float4 *n = s.node + 4 * (size_t)t.node;
+      if (kCount) tc->nodes++;
+      const float4 a = __ldg(n + 0), b = __ldg(n + 1), c = __ldg(n + 2);
+      const int4 l = __ldg(reinterpret_cast<const int4 *>(n) + 3);
+      float e0, x0, e1, x1;
+      box_hit(a.x, a.y, a.z, a.w, c.x, c.y, t.o, t.inv, e0, x0);
+      box_hit(b.x, b.y, b.z, b.w, c.z, c.w, t.o, t.inv, e1, x1);
+      const bool h0 = e0 < x0 && x0 > 0.f && e0 <= t.tcull;
+      const bool h1 = e1 < x1 && x1 > 0.f && e1 <= t.tcull;
+      if (h0 && h1) {
+        int nr = l.x, fr = l.y;
+        float fe = e1;
+        if (e1 < e0) { nr = l.y; fr = l.x; fe = e0; }
+        if (t.sp < kStackDepth) stack[t.sp++] = make_int2(fr, __float_as_int(fe));
+        else errbits |= kErrStackOverflow;
+        t.node = nr;
+      } else if (h0) {
+        t.node = l.x;
+      } else if (h1) {
+        t.node = l.y;
+      } else {
+        t.node = kTravDone;
+        while (t.sp > 0) {
+          const int2 e = stack[--t.sp];
+          if (__int_as_float(e.y) <= t.tcull) { t.node = e.x; break; }
+        }
+      }
+      // postpone the first leaf found and keep descending from the stack
+      if (t.node < 0 && t.node != kTravDone && leaf == 0) {
+        leaf = t.node;
+        t.node = kTravDone;
+        while (t.sp > 0) {
+          const int2 e = stack[--t.sp];
+          if (__int_as_float(e.y) <= t.tcull) { t.node = e.x; break; }
+        }
+      }
+      if (!__any_sync(__activemask(), leaf == 0)) break;
+    }
+    // ---- leaves
+    for (;;) {
+      int code = 0;
+      if (leaf < 0) {
+        code = ~leaf;
+        leaf = 0;
+      } else if (t.node < 0 && t.node != kTravDone) {
+        code = ~t.node;
+        t.node = kTravDone;
+        while (t.sp > 0) {
+          const int2 e = stack[--t.sp];
+          if (__int_as_float(e.y) <= t.tcull) { t.node = e.x; break; }
+        }
+      } else {
+        break;
+      }
+      const int first = code >> 4;
+      const int cnt = (code & 15) + 1;
+      if (kCount) tc->tris += cnt;
+      for (int i = 0; i < cnt; ++i) {
+        const float4 *tp = s.tri + 3 * (size_t)(first + i);
+        const float4 A = __ldg(tp + 0), E1 = __ldg(tp + 1), E2 = __ldg(tp + 2);
+        float u, v;
+        const float tt = tri_hit(t.o, t.d, A, E1, E2, eps, u, v);
+        if (tt > eps && tt < t.h.t) {
+          t.h.t = tt;
+          t.h.u = u;
+          t.h.v = v;
+          t.h.slot = first + i;
+          t.tcull = fminf(t.tcull, cull_bound(tt));
+        }
+      }
+    }
+    if (t.node == kTravDone && leaf == 0) return true;
+  }
+  return t.node == kTravDone && leaf == 0;
+}
+
+// ---- wide nodes (4 or 8 children) ---------------------------------------
+template <int W>
+TS_D void cswap(float *k, int *r, int i, int j) {
+  if (k[j] < k[i]) {
+    const float tk = k[i];
+    k[i] = k[j];
+    k[j] = tk;
+    const int tr = r[i];
+    r[i] = r[j];
+    r[j] = tr;
+  }
+}
+
+// Sort W (entry distance, link) pairs ascending (misses carry +inf):
+// 5-comparator network for 4, Batcher's 19-comparator network for 8.
+template <int W>
+TS_D void sort_children(float *k, int *r) {
+  if (W == 4) {
+    cswap<W>(k, r, 0, 1); cswap<W>(k, r, 2, 3); cswap<W>(k, r, 0, 2); cswap<W>(k, r, 1, 3); cswap<W>(k, r, 1, 2);
+  } else {
+    cswap<W>(k, r, 0, 1); cswap<W>(k, r, 2, 3); cswap<W>(k, r, 4, 5); cswap<W>(k, r, 6, 7);
+    cswap<W>(k, r, 0, 2); cswap<W>(k, r, 1, 3); cswap<W>(k, r, 4, 6); cswap<W>(k, r, 5, 7);
+    cswap<W>(k, r, 1, 2); cswap<W>(k, r, 5, 6);
+    cswap<W>(k, r, 0, 4); cswap<W>(k, r, 1, 5); cswap<W>(k, r, 2, 6); cswap<W>(k, r, 3, 7);
+    cswap<W>(k, r, 2, 4); cswap<W>(k, r, 3, 5);
+    cswap<W>(k, r, 1, 2); cswap<W>(k, r, 3, 4); cswap<W>(k, r, 5, 6);
+  }
+}
+
+// Same contract as trav_steps, for the wide layout: the children a node's
+// ray enters are sorted by entry distance; the nearest is visited next and
+// the others are pushed (farthest first) with their entry distances.
+template <int W, bool kCount = false>
+TS_D bool trav_steps_wide(const DevScene &s, Traversal &t, int2 *stack, float eps, int budget, uint32_t &errbits,
+                          TraceCount *tc = nullptr) {
+  constexpr int P = W / 4;  // float4s per row
+  for (int it = 0; it < budget; ++it) {
+    if (t.node == kTravDone) return true;
+    if (t.node >= 0) {
+      const float4 *n = s.node + (size_t)(6 * P + P + (W == 4 ? 1 : 2)) * t.node;
+      if (kCount) tc->nodes++;
+      float row[6][W];
+#pragma unroll
+      for (int r = 0; r < 6; ++r)
+#pragma unroll
+        for (int q = 0; q < P; ++q) {
+          const float4 v = __ldg(n + r * P + q);
+          row[r][4 * q + 0] = v.x; row[r][4 * q + 1] = v.y; row[r][4 * q + 2] = v.z; row[r][4 * q + 3] = v.w;
+        }
+      int ref[W];
+#pragma unroll
+      for (int q = 0; q < P; ++q) {
+        const int4 l = __ldg(reinterpret_cast<const int4 *>(n + 6 * P + q));
+        ref[4 * q + 0] = l.x; ref[4 * q + 1] = l.y; ref[4 * q + 2] = l.z; ref[4 * q + 3] = l.w;
+      }
+      float key[W];
+      int nh = 0;
+#pragma unroll
+      for (int k = 0; k < W; ++k) {
+        float te, tx;
+        box_hit(row[0][k], row[1][k], row[2][k], row[3][k], row[4][k], row[5][k], t.o, t.inv, te, tx);
+        const bool h = te < tx && tx > 0.f && te <= t.tcull;
+        key[k] = h ? te : INFINITY;
+        nh += h;
+      }
+      if (nh > 0) {
+        sort_children<W>(key, ref);
+        if (t.sp + nh - 1 <= kWideStack) {
+#pragma unroll
+          for (int k = W - 1; k >= 1; --k)
+            if (k < nh) stack[t.sp++] = make_int2(ref[k], __float_as_int(key[k]));
+        } else {
+          errbits |= kErrStackOverflow;
+        }
+        t.node = ref[0];
+        continue;
+      }
+    } else {
+      const int code = ~t.node;
+      const int first = code >> 4;
+      const int cnt = (code & 15) + 1;
+      if (kCount) tc->tris += cnt;
+      for (int i = 0; i < cnt; ++i) {
+        const float4 *tp = s.tri + 3 * (size_t)(first + i);
+        const float4 A = __ldg(tp + 0), E1 = __ldg(tp + 1), E2 = __ldg(tp + 2);
+        float u, v;
+        const float tt = tri_hit(t.o, t.d, A, E1, E2, eps, u, v);
+        if (tt > eps && tt < t.h.t) {
+          t.h.t = tt;
+          t.h.u = u;
+          t.h.v = v;
+          t.h.slot = first + i;
+          t.tcull = fminf(t.tcull, cull_bound(tt));
+        }
+      }
+    }
+    for (;;) {
+      if (t.sp == 0) {
+        t.node = kTravDone;
+        return true;
+      }
+      const int2 e = stack[--t.sp];
+      if (__int_as_float(e.y) <= t.tcull) {
+        t.node = e.x;
+        break;
+      }
+    }
+  }
+  return t.node == kTravDone;
+}
+
+// Dispatch on the node width (a compile-time choice of each kernel instance).
+// W = 2: two-child if-if loop; W = 3: two-child speculative while-while (same
+// layout); W = 4 / 8: wide nodes.
+template <int W, bool kCount = false>
+TS_D bool trav_advance(const DevScene &s, Traversal &t, int2 *stack, float eps, int budget, uint32_t &errbits,
+                       TraceCount *tc = nullptr) {
+  if (W == 2) return trav_steps<kCount>(s, t, stack, eps, budget, errbits, tc);
+  if (W == 3) return trav_steps_spec<kCount>(s, t, stack, eps, budget, errbits, tc);
+  return trav_steps_wide<W, kCount>(s, t, stack, eps, budget, errbits, tc);
+}
+
+template <int W>
+struct StackSize {
+  static constexpr int value = W <= 3 ? kStackDepth : kWideStack;
+};
+
+// Fast closest hit in one go (local-memory stack).  errbits gets
+// kErrStackOverflow if the tree is deeper than the stack (the builder bounds
+// the depth below it, so this is a guard only).
+template <int W, bool kCount = false>
+TS_D Hit trace_closest(const DevScene &s, float3 o, float3 d, float eps, uint32_t &errbits, TraceCount *tc = nullptr,
+                       float bound = 1e9f) {
+  Traversal t;
+  int2 stack[StackSize<W>::value];
+  trav_begin(s, t, o, d, bound);
+  trav_advance<W, kCount>(s, t, stack, eps, 0x7fffffff, errbits, tc);
+  return t.h;
 }
 
 // Exact reference-order closest hit on the reference-layout table.

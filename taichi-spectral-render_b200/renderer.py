@@ -52,6 +52,8 @@ class RenderConfig:
     block_size: int = 0
     blocks_per_sm: int = 0
     sort_keys: int = 0
+    trace_budget: int = 0
+    traversal: str = "default"      # two-child nodes: "default" (if-if loop) or "speculative" (while-while)
     device: int = 0
 
     @property
@@ -71,6 +73,8 @@ class RenderConfig:
         c.seed, c.scene_id, c.device = self.seed & 0xFFFFFFFF, self.scene_id & 0xFFFFFFFF, self.device
         c.kernel = {"mega": _lib.KERNEL_MEGA, "wavefront": _lib.KERNEL_WAVEFRONT}[self.kernel]
         c.block_size, c.blocks_per_sm, c.sort_keys = self.block_size, self.blocks_per_sm, self.sort_keys
+        c.trace_budget = self.trace_budget
+        c.traversal = {"default": 0, "speculative": 1}[self.traversal]
         return c
 
 

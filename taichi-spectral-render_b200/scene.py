@@ -176,6 +176,7 @@ class CompiledScene:
         d.bvh_leaf_max = int(p.get("leaf_max", 0))
         d.bvh_cost_trav = float(p.get("cost_trav", 0.0))
         d.bvh_cost_tri = float(p.get("cost_tri", 0.0))
+        d.bvh_width = int(p.get("width", 0))
         return d
 
 

@@ -27,9 +27,10 @@ def oracle_passes(comp, bvh, scene, cfg, passes, use_double=False):
     return out
 
 
-def gpu_passes(scene, cfg, ex, bvh, kernel, passes, sort_keys=0):
-    c2 = sb.RenderConfig(**{**cfg.__dict__, "kernel": kernel, "sort_keys": sort_keys})
-    with sb.Renderer(scene, c2, eems=ex["eems"], cmf=ex["cmf"], bvh=bvh) as r:
+def gpu_passes(scene, cfg, ex, bvh, kernel, passes, sort_keys=0, node_width=0, traversal="default"):
+    c2 = sb.RenderConfig(**{**cfg.__dict__, "kernel": kernel, "sort_keys": sort_keys, "traversal": traversal})
+    with sb.Renderer(scene, c2, eems=ex["eems"], cmf=ex["cmf"], bvh=bvh,
+                     bvh_params={"width": node_width}) as r:
         for p in passes:
             r.cast_rays(p % cfg.bands, pass_idx=p)
         g = r.block_film.cpu().numpy().reshape(cfg.bands, -1).T.copy()
@@ -49,19 +50,21 @@ def crn_agreement(g, o):
     assert close.mean() > 0.995, close.mean()
 
 
-@pytest.mark.parametrize("kernel", ["mega", "wavefront"])
-def test_box_scene_common_random_numbers(kernel):
+@pytest.mark.parametrize("kernel,node_width", [("mega", 2), ("wavefront", 2), ("mega", 4), ("wavefront", 8)])
+def test_box_scene_common_random_numbers(kernel, node_width):
     s, c, ex, comp, bvh = setup(configs.box_scene, width=48, height=48)
     passes = range(25)
-    crn_agreement(gpu_passes(s, c, ex, bvh, kernel, passes), oracle_passes(comp, bvh, s, c, passes))
+    crn_agreement(gpu_passes(s, c, ex, bvh, kernel, passes, node_width=node_width),
+                  oracle_passes(comp, bvh, s, c, passes))
 
 
-@pytest.mark.parametrize("kernel", ["mega", "wavefront"])
-def test_volume_fluorescence_common_random_numbers(kernel):
+@pytest.mark.parametrize("kernel,node_width", [("mega", 2), ("wavefront", 4), ("mega", 8)])
+def test_volume_fluorescence_common_random_numbers(kernel, node_width):
     s, c, ex, comp, bvh = setup(configs.volume_scene, width=40, height=40, medium_slices=30, medium_stacks=31,
                                 fluorescent_medium=True, depth=16)
     passes = range(25)
-    crn_agreement(gpu_passes(s, c, ex, bvh, kernel, passes), oracle_passes(comp, bvh, s, c, passes))
+    crn_agreement(gpu_passes(s, c, ex, bvh, kernel, passes, node_width=node_width),
+                  oracle_passes(comp, bvh, s, c, passes))
 
 
 def test_reference_scene_common_random_numbers():
@@ -89,8 +92,17 @@ def test_wavefront_equals_megakernel():
     a = gpu_passes(s, c, ex, bvh, "mega", passes)
     b = gpu_passes(s, c, ex, bvh, "wavefront", passes)
     d = gpu_passes(s, c, ex, bvh, "wavefront", passes, sort_keys=1)
-    assert np.allclose(a, b, rtol=1e-12, atol=1e-12)
-    assert np.allclose(a, d, rtol=1e-12, atol=1e-12)
+    # the same paths (no multiply-add contraction anywhere); only the order of
+    # the FP64 film additions differs between the two kernels
+    assert np.allclose(a, b, rtol=1e-12, atol=1e-15)
+    # the shading order of a queue never changes a path
+    assert np.array_equal(b, d)
+    # node widths and traversal loops change only which boxes are opened, never a result
+    for w in (4, 8):
+        e = gpu_passes(s, c, ex, bvh, "wavefront", passes, node_width=w)
+        assert np.array_equal(b, e), w
+    assert np.array_equal(b, gpu_passes(s, c, ex, bvh, "wavefront", passes, traversal="speculative"))
+    assert np.array_equal(a, gpu_passes(s, c, ex, bvh, "mega", passes, traversal="speculative"))
 
 
 def test_statistical_parity_three_sigma():
