@@ -26,7 +26,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 # algorithmic bytes of one unit of work, for the roofline (layouts in csrc/common.cuh)
-BYTES_NODE = 64      # one two-child BVH node (two child boxes + links)
+BYTES_NODE = 64      # one two-child BVH node (two child boxes + links); wide nodes 128 / 256 B
 BYTES_TRI = 48       # one triangle test (v0, e1, e2 as float4)
 BYTES_HIT = 48       # shading normals of a resolved hit (3 float4)
 BYTES_MAT_VERTEX = 8 * 32  # material lookups per path vertex (8 x two float4)
@@ -244,7 +244,8 @@ def bench_ours(args):
         r.cast_rays(w % B, pass_idx=base_pass + w)
     work = r.cast_rays_counted(12, pass_idx=base_pass + args.warmup)
     torch.cuda.synchronize()
-    bytes_per_path = (BYTES_NODE * work["node_visits"] + BYTES_TRI * work["tri_tests"] + BYTES_HIT * work["hits"]
+    node_bytes = BYTES_NODE * (args.width // 2)  # 2 -> 64 B, 4 -> 128 B, 8 -> 256 B
+    bytes_per_path = (node_bytes * work["node_visits"] + BYTES_TRI * work["tri_tests"] + BYTES_HIT * work["hits"]
                       + BYTES_MAT_VERTEX * work["vertices"] + BYTES_DEPOSIT * work["deposits"]) / work["paths"]
 
     # ---- timed region: K passes, device time, max over ranks

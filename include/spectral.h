@@ -57,7 +57,8 @@ typedef struct {
   int32_t kernel;                /* TS_KERNEL_MEGA or TS_KERNEL_WAVEFRONT */
   int32_t block_size;            /* threads per block of the render kernels, 32..256 (0 = 128) */
   int32_t blocks_per_sm;         /* persistent grid = SMs * blocks_per_sm (0 = default) */
-  int32_t sort_keys;             /* wavefront: sort shading queue by material (0 = off) */
+  int32_t sort_keys;             /* wavefront queue sorting, bit mask: 1 shading queue by material,
+                                    2 extension rays by direction octant, 4 shadow rays by light (0 = off) */
   int32_t trace_budget;          /* wavefront: traversal steps between refills of idle lanes (0 = 32) */
   int32_t traversal;             /* TS_TRAVERSAL_DEFAULT or TS_TRAVERSAL_SPECULATIVE (two-child nodes) */
 } ts_config;

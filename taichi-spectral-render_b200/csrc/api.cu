@@ -651,6 +651,8 @@ static ts_status ensure_wave(ts_ctx *c) {
   TS_CUDA(c, grab((void **)&w.queue[1], N * sizeof(int)), "wavefront buffers");
   TS_CUDA(c, grab((void **)&w.shadow_queue, N * sizeof(int)), "wavefront buffers");
   TS_CUDA(c, grab((void **)&w.sorted, N * sizeof(int)), "wavefront buffers");
+  TS_CUDA(c, grab((void **)&w.trace_order, N * sizeof(int)), "wavefront buffers");
+  TS_CUDA(c, grab((void **)&w.shadow_order, N * sizeof(int)), "wavefront buffers");
   TS_CUDA(c, grab((void **)&w.counts, 8192 * sizeof(int)), "wavefront buffers");
   TS_CUDA(c, grab((void **)&w.key_hist, 2 * ts::kMaxKeys * sizeof(int)), "wavefront buffers");
   w.capacity = n;

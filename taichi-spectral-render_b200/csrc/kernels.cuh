@@ -47,7 +47,9 @@ struct WaveBuffers {
   int4 *sq_meta;      // (pixel, light_slot, vol, band)
   int *queue[2];      // extension queues (ping-pong), path ids
   int *shadow_queue;  // shadow queue, query ids == path ids
-  int *sorted;        // extension queue ordered by material key
+  int *sorted;        // extension queue ordered by material key (shading)
+  int *trace_order;   // extension queue ordered by direction octant (tracing)
+  int *shadow_order;  // shadow query indices ordered by light triangle
   int *counts;        // [2*max_depth + 8]: ext counts per depth, shadow counts per depth, scratch
   int *key_hist;      // material-key histogram / offsets [kMaxKeys * 2]
   int capacity;

@@ -78,11 +78,12 @@ __global__ void k_generate(DevScene s, DevConfig c, uint32_t pass, int band, Wav
 // items (one atomic per warp), so a warp does not idle behind its longest ray.
 template <int W>
 __global__ void __launch_bounds__(kMaxBlock, 4) k_trace(DevScene s, DevConfig c, int depth, Film f, WaveBuffers w,
-                                                     uint32_t *__restrict__ err, int budget) {
+                                                     uint32_t *__restrict__ err, int budget, int ext_sorted,
+                                                     int shadow_sorted) {
   uint32_t eb = 0;
   const int nsh = depth > 0 ? w.counts[kCntSh + depth - 1] : 0;
   const int next = depth < c.max_depth ? w.counts[kCntExt + depth] : 0;
-  const int *q = w.queue[depth & 1];
+  const int *q = ext_sorted ? w.trace_order : w.queue[depth & 1];
   const int total = nsh + next;
   int *fetch = w.counts + kCntFetchT + depth;
   const int lane = threadIdx.x & 31;
@@ -106,8 +107,9 @@ __global__ void __launch_bounds__(kMaxBlock, 4) k_trace(DevScene s, DevConfig c,
           exhausted = true;
         } else if (idx < nsh) {
           item = idx;
-          const float4 o = w.sq_origin[idx], d = w.sq_dir[idx];
-          const int4 mm = w.sq_meta[idx];
+          const int qi = shadow_sorted ? w.shadow_order[idx] : idx;
+          const float4 o = w.sq_origin[qi], d = w.sq_dir[qi];
+          const int4 mm = w.sq_meta[qi];
           sq.origin = xyz(o);
           sq.max_dist = o.w;
           sq.dir = xyz(d);
@@ -150,28 +152,55 @@ __global__ void __launch_bounds__(kMaxBlock, 4) k_trace(DevScene s, DevConfig c,
 }
 
 void launch_trace(const DevScene &s, const DevConfig &c, int depth, Film f, const WaveBuffers &w, uint32_t *err,
-                  int grid, int block, cudaStream_t st, int budget) {
-  if (s.node_width == 8) k_trace<8><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget);
-  else if (s.node_width == 4) k_trace<4><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget);
-  else if (c.speculative) k_trace<3><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget);
-  else k_trace<2><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget);
+                  int grid, int block, cudaStream_t st, int budget, int ext_sorted = 0, int shadow_sorted = 0) {
+  if (s.node_width == 8)
+    k_trace<8><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget, ext_sorted, shadow_sorted);
+  else if (s.node_width == 4)
+    k_trace<4><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget, ext_sorted, shadow_sorted);
+  else if (c.speculative)
+    k_trace<3><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget, ext_sorted, shadow_sorted);
+  else
+    k_trace<2><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget, ext_sorted, shadow_sorted);
 }
 
-// material key of a queued path for the shading sort (num_materials = miss)
-__device__ __forceinline__ int shade_key(const DevScene &s, const WaveBuffers &w, int pid, int nkeys) {
-  const int slot = __float_as_int(w.hit[pid].w);
-  int key = slot >= 0 ? __float_as_int(__ldg(s.tri + 3 * (size_t)slot + 1).w) : s.num_materials;
-  return key < nkeys ? key : nkeys - 1;
+// ---- queue sorting ------------------------------------------------------
+// Counting sorts that reorder a queue by a small key so that neighbouring
+// lanes of a warp take similar work: the shading queue by hit material, the
+// extension rays by direction octant, the shadow queries by light triangle.
+// Each is count (block histograms) -> scan -> scatter (one atomic per key per
+// warp, lanes of equal keys grouped with __match_any_sync).
+enum SortKind { kSortShade = 0, kSortExt = 1, kSortShadow = 2 };
+constexpr int kExtKeys = 8, kShadowKeys = 16;
+
+__device__ __forceinline__ int sort_count_of(const WaveBuffers &w, int kind, int depth) {
+  return kind == kSortShadow ? w.counts[kCntSh + depth] : w.counts[kCntExt + depth];
 }
 
-__global__ void k_sort_count(DevScene s, DevConfig c, int depth, WaveBuffers w, int nkeys) {
+__device__ __forceinline__ int sort_item(const WaveBuffers &w, int kind, int depth, int i) {
+  return kind == kSortShadow ? i : w.queue[depth & 1][i];
+}
+
+__device__ __forceinline__ int sort_key(const DevScene &s, const WaveBuffers &w, int kind, int item, int nkeys) {
+  int key;
+  if (kind == kSortShade) {
+    const int slot = __float_as_int(w.hit[item].w);
+    key = slot >= 0 ? __float_as_int(__ldg(s.tri + 3 * (size_t)slot + 1).w) : s.num_materials;
+  } else if (kind == kSortExt) {
+    const float4 d = w.dir_spdf[item];
+    key = (d.x < 0.f ? 1 : 0) | (d.y < 0.f ? 2 : 0) | (d.z < 0.f ? 4 : 0);
+  } else {
+    key = w.sq_meta[item].y;
+  }
+  return kind == kSortShade ? (key < nkeys ? key : nkeys - 1) : (key & (nkeys - 1));
+}
+
+__global__ void k_sort_count(DevScene s, int depth, WaveBuffers w, int kind, int nkeys) {
   __shared__ int hist[kMaxKeys];
   for (int k = threadIdx.x; k < nkeys; k += blockDim.x) hist[k] = 0;
   __syncthreads();
-  const int n = w.counts[kCntExt + depth];
-  const int *q = w.queue[depth & 1];
+  const int n = sort_count_of(w, kind, depth);
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    atomicAdd(&hist[shade_key(s, w, q[i], nkeys)], 1);
+    atomicAdd(&hist[sort_key(s, w, kind, sort_item(w, kind, depth, i), nkeys)], 1);
   __syncthreads();
   for (int k = threadIdx.x; k < nkeys; k += blockDim.x)
     if (hist[k]) atomicAdd(&w.key_hist[k], hist[k]);
@@ -183,20 +212,37 @@ __global__ void k_sort_scan(WaveBuffers w, int nkeys) {
     for (int k = 0; k < nkeys; ++k) {
       const int v = w.key_hist[k];
       w.key_hist[kMaxKeys + k] = run;  // running insert position
-      w.key_hist[k] = 0;               // cleared for the next depth
+      w.key_hist[k] = 0;               // cleared for the next sort
       run += v;
     }
   }
 }
 
-__global__ void k_sort_scatter(DevScene s, DevConfig c, int depth, WaveBuffers w, int nkeys) {
-  const int n = w.counts[kCntExt + depth];
-  const int *q = w.queue[depth & 1];
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const int pid = q[i];
-    const int pos = atomicAdd(&w.key_hist[kMaxKeys + shade_key(s, w, pid, nkeys)], 1);
-    w.sorted[pos] = pid;
+__global__ void k_sort_scatter(DevScene s, int depth, WaveBuffers w, int kind, int nkeys, int *__restrict__ out) {
+  const int n = sort_count_of(w, kind, depth);
+  const int lane = threadIdx.x & 31;
+  const int stride = gridDim.x * blockDim.x;
+  for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
+    const int i = base + lane;
+    const bool valid = i < n;
+    const unsigned active = __ballot_sync(0xffffffffu, valid);
+    if (!valid) continue;
+    const int item = sort_item(w, kind, depth, i);
+    const int key = sort_key(s, w, kind, item, nkeys);
+    const unsigned peers = __match_any_sync(active, key);
+    const int leader = __ffs(peers) - 1;
+    int pos = 0;
+    if (lane == leader) pos = atomicAdd(&w.key_hist[kMaxKeys + key], __popc(peers));
+    pos = __shfl_sync(peers, pos, leader);
+    out[pos + __popc(peers & ((1u << lane) - 1u))] = item;
   }
+}
+
+void launch_sort(const DevScene &s, int depth, const WaveBuffers &w, int kind, int nkeys, int *out, int grid,
+                 cudaStream_t st) {
+  k_sort_count<<<grid, 256, 0, st>>>(s, depth, w, kind, nkeys);
+  k_sort_scan<<<1, 32, 0, st>>>(w, nkeys);
+  k_sort_scatter<<<grid, 256, 0, st>>>(s, depth, w, kind, nkeys, out);
 }
 
 __global__ void __launch_bounds__(kMaxBlock) k_shade(DevScene s, DevConfig c, uint32_t pass, int band, int depth,
@@ -297,22 +343,29 @@ cudaError_t launch_wave_pass(const DevScene &s, const DevConfig &c, uint32_t pas
   const int npix = c.W * c.H;
   const int gen_grid = (npix + 255) / 256;
   k_generate<<<gen_grid, 256, 0, st>>>(s, c, pass, band, w);
-  const int nkeys = sort_keys ? (s.num_materials + 1 < kMaxKeys ? s.num_materials + 1 : kMaxKeys) : 0;
-  if (nkeys) {
+  // sort_keys bit 0: shading queue by material; bit 1: extension rays by
+  // direction octant; bit 2: shadow queries by light triangle
+  const int nmat = s.num_materials + 1 < kMaxKeys ? s.num_materials + 1 : kMaxKeys;
+  if (sort_keys) {
     e = cudaMemsetAsync(w.key_hist, 0, 2 * kMaxKeys * sizeof(int), st);
     if (e != cudaSuccess) return e;
   }
+  const int sort_grid = grid < 4 * 148 ? grid : 4 * 148;
   for (int d = 0; d < c.max_depth; ++d) {
-    launch_trace(s, c, d, f, w, err, grid, block, st, trace_budget);
-    if (nkeys) {
-      k_sort_count<<<grid, 256, 0, st>>>(s, c, d, w, nkeys);
-      k_sort_scan<<<1, 32, 0, st>>>(w, nkeys);
-      k_sort_scatter<<<grid, 256, 0, st>>>(s, c, d, w, nkeys);
-    }
-    k_shade<<<grid, block, 0, st>>>(s, c, pass, band, d, f, w, nkeys ? 1 : 0);
+    const int ext_sorted = (sort_keys & 2) ? 1 : 0;
+    const int sh_sorted = (sort_keys & 4) && d > 0 ? 1 : 0;
+    if (ext_sorted) launch_sort(s, d, w, kSortExt, kExtKeys, w.trace_order, sort_grid, st);
+    if (sh_sorted) launch_sort(s, d - 1, w, kSortShadow, kShadowKeys, w.shadow_order, sort_grid, st);
+    launch_trace(s, c, d, f, w, err, grid, block, st, trace_budget, ext_sorted, sh_sorted);
+    if (sort_keys & 1) launch_sort(s, d, w, kSortShade, nmat, w.sorted, sort_grid, st);
+    k_shade<<<grid, block, 0, st>>>(s, c, pass, band, d, f, w, (sort_keys & 1) ? 1 : 0);
   }
   // the last depth's shadow queries
-  if (c.max_depth > 0) launch_trace(s, c, c.max_depth, f, w, err, grid, block, st, trace_budget);
+  if (c.max_depth > 0) {
+    const int sh_sorted = (sort_keys & 4) ? 1 : 0;
+    if (sh_sorted) launch_sort(s, c.max_depth - 1, w, kSortShadow, kShadowKeys, w.shadow_order, sort_grid, st);
+    launch_trace(s, c, c.max_depth, f, w, err, grid, block, st, trace_budget, 0, sh_sorted);
+  }
   return cudaGetLastError();
 }
 

@@ -95,8 +95,10 @@ def test_wavefront_equals_megakernel():
     # the same paths (no multiply-add contraction anywhere); only the order of
     # the FP64 film additions differs between the two kernels
     assert np.allclose(a, b, rtol=1e-12, atol=1e-15)
-    # the shading order of a queue never changes a path
+    # the order of a queue (shading by material; tracing by octant and by
+    # light) never changes a path
     assert np.array_equal(b, d)
+    assert np.array_equal(b, gpu_passes(s, c, ex, bvh, "wavefront", passes, sort_keys=7))
     # node widths and traversal loops change only which boxes are opened, never a result
     for w in (4, 8):
         e = gpu_passes(s, c, ex, bvh, "wavefront", passes, node_width=w)
