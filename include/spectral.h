@@ -178,6 +178,29 @@ ts_status ts_trace_batch(ts_ctx *ctx, const float *rays_dev, int32_t n, int32_t 
 /* normals_dev: [H][W][3] float32 */
 ts_status ts_render_normals(ts_ctx *ctx, float *normals_dev, void *stream);
 
+/* ---- differentiation (new; the reference renders forward only).
+ * Parameters are the material table [M][6][B] of ts_scene_desc.mat_f32
+ * (main.py:545-561) followed by the EEM table [E][B][B]; gradients exist for
+ * every entry except the refractive index (property 0), which bends rays.
+ * Counts: M*6*B material entries, E*B*B EEM entries. */
+ts_status ts_param_count(const ts_ctx *ctx, int64_t *num_material_params, int64_t *num_eem_params);
+
+/* Replace the material and/or EEM tables (device arrays in the ts_scene_desc
+ * layout; either may be NULL) without touching geometry, BVH or lights: the
+ * parameter update of an optimiser.  The integer flags (is_true_volume,
+ * surface_emission) and EEM ids stay as uploaded.  Stream-ordered. */
+ts_status ts_update_materials(ts_ctx *ctx, const float *mat_f32_dev, const float *eem_dev, void *stream);
+
+/* Path-replay adjoint of ts_render_pass(pass_idx, band): re-runs each path of
+ * that pass from its random stream and ADDS into grad_dev ([M*6*B + E*B*B]
+ * float64, device) the derivative of sum over the pass's film deposits of
+ * adj[band'][j][i] * deposit, where adj_dev is a [B][H][W] float64 device
+ * array (dLoss/d film cell).  Sampling decisions that depend on a parameter
+ * contribute their score terms, so the result is the gradient of the expected
+ * pass.  scatter_bounces must be <= 16. */
+ts_status ts_adjoint_pass(ts_ctx *ctx, uint32_t pass_idx, int32_t band, const double *adj_dev, double *grad_dev,
+                          void *stream);
+
 /* ---- device status: error bits raised by kernels since the last call (synchronises) */
 ts_status ts_check_device(ts_ctx *ctx, uint32_t *bits);
 

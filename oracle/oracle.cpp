@@ -20,6 +20,7 @@
 #include "oracle.h"
 
 #include <algorithm>
+#include <type_traits>
 #include <cmath>
 #include <cstring>
 #include <numeric>
@@ -29,6 +30,104 @@
 #endif
 
 namespace {
+
+using std::acos;
+using std::cos;
+using std::exp;
+using std::fabs;
+using std::fmax;
+using std::fmin;
+using std::log;
+using std::max;
+using std::min;
+using std::sin;
+using std::sqrt;
+using std::tan;
+
+// ---------------------------------------------------------------- forward-mode duals
+// The adjoint oracle instantiates the estimator with Dual<double, kDualN>: a
+// value and its partial derivatives with respect to up to kDualN selected
+// material / EEM parameters.  Branches compare values only, so the value part
+// follows the FP64 estimator operation for operation.
+constexpr int kDualN = 16;
+template <class T, int K> struct Dual {
+  T v;
+  T d[K];
+  Dual() : v(0) { for (int i = 0; i < K; ++i) d[i] = 0; }
+  template <class S, class = typename std::enable_if<std::is_arithmetic<S>::value>::type>
+  Dual(S x) : v(T(x)) { for (int i = 0; i < K; ++i) d[i] = 0; }
+  explicit operator double() const { return double(v); }
+  explicit operator float() const { return float(v); }
+  friend Dual operator+(const Dual &a, const Dual &b) {
+    Dual r; r.v = a.v + b.v; for (int i = 0; i < K; ++i) r.d[i] = a.d[i] + b.d[i]; return r;
+  }
+  friend Dual operator-(const Dual &a, const Dual &b) {
+    Dual r; r.v = a.v - b.v; for (int i = 0; i < K; ++i) r.d[i] = a.d[i] - b.d[i]; return r;
+  }
+  friend Dual operator-(const Dual &a) {
+    Dual r; r.v = -a.v; for (int i = 0; i < K; ++i) r.d[i] = -a.d[i]; return r;
+  }
+  friend Dual operator*(const Dual &a, const Dual &b) {
+    Dual r; r.v = a.v * b.v; for (int i = 0; i < K; ++i) r.d[i] = a.d[i] * b.v + a.v * b.d[i]; return r;
+  }
+  friend Dual operator/(const Dual &a, const Dual &b) {
+    Dual r; r.v = a.v / b.v; for (int i = 0; i < K; ++i) r.d[i] = (a.d[i] - r.v * b.d[i]) / b.v; return r;
+  }
+  Dual &operator+=(const Dual &b) { return *this = *this + b; }
+  Dual &operator-=(const Dual &b) { return *this = *this - b; }
+  Dual &operator*=(const Dual &b) { return *this = *this * b; }
+  friend bool operator<(const Dual &a, const Dual &b) { return a.v < b.v; }
+  friend bool operator>(const Dual &a, const Dual &b) { return a.v > b.v; }
+  friend bool operator<=(const Dual &a, const Dual &b) { return a.v <= b.v; }
+  friend bool operator>=(const Dual &a, const Dual &b) { return a.v >= b.v; }
+  friend bool operator==(const Dual &a, const Dual &b) { return a.v == b.v; }
+  friend bool operator!=(const Dual &a, const Dual &b) { return a.v != b.v; }
+  // chain rule for a unary function with value fv and derivative df at a.v
+  static Dual chain(const Dual &a, T fv, T df) {
+    Dual r; r.v = fv; for (int i = 0; i < K; ++i) r.d[i] = a.d[i] * df; return r;
+  }
+  friend Dual sqrt(const Dual &a) {
+    const T r = std::sqrt(a.v);
+    return chain(a, r, r > T(0) ? T(0.5) / r : T(0));
+  }
+  friend Dual exp(const Dual &a) { const T e = std::exp(a.v); return chain(a, e, e); }
+  friend Dual log(const Dual &a) { return chain(a, std::log(a.v), T(1) / a.v); }
+  friend Dual acos(const Dual &a) {
+    const T q = T(1) - a.v * a.v;
+    return chain(a, std::acos(a.v), q > T(0) ? -T(1) / std::sqrt(q) : T(0));
+  }
+  friend Dual cos(const Dual &a) { return chain(a, std::cos(a.v), -std::sin(a.v)); }
+  friend Dual sin(const Dual &a) { return chain(a, std::sin(a.v), std::cos(a.v)); }
+  friend Dual tan(const Dual &a) { const T t = std::tan(a.v); return chain(a, t, T(1) + t * t); }
+  friend Dual fabs(const Dual &a) { return a.v < T(0) ? -a : a; }
+  friend Dual max(const Dual &a, const Dual &b) { return a < b ? b : a; }
+  friend Dual min(const Dual &a, const Dual &b) { return b < a ? b : a; }
+  friend Dual fmax(const Dual &a, const Dual &b) { return (b.v > a.v || a.v != a.v) ? b : a; }
+  friend Dual fmin(const Dual &a, const Dual &b) { return (b.v < a.v || a.v != a.v) ? b : a; }
+};
+template <class R> struct is_dual : std::false_type {};
+template <class T, int K> struct is_dual<Dual<T, K>> : std::true_type {};
+
+// A sampled value enters the estimator as a fixed number: its dependence on
+// the parameters is accounted for by the score of its density instead.
+template <class R> inline R detach(const R &a) {
+  if constexpr (is_dual<R>::value) return R(a.v);
+  else return a;
+}
+// Score factor of a sampling decision with probability (density) p: value
+// exactly 1, derivative d log p.  Multiplied into the estimate of the event,
+// it adds d log p times every later deposit.  Plain types: no factor at all.
+template <class R> inline void apply_score(R &est, const R &p) {
+  if constexpr (is_dual<R>::value) {
+    if (!(p.v > 0)) return;
+    R s(1.0);
+    for (int i = 0; i < kDualN; ++i) s.d[i] = p.d[i] / p.v;
+    est = est * s;
+  } else {
+    (void)est;
+    (void)p;
+  }
+}
 
 // ---------------------------------------------------------------- Philox
 inline void philox_block(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
@@ -79,20 +178,21 @@ template <class R> inline R dot(V3<R> a, V3<R> b) { return a.x * b.x + a.y * b.y
 template <class R> inline V3<R> cross(V3<R> a, V3<R> b) {
   return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
 }
-template <class R> inline R norm(V3<R> a) { return std::sqrt(dot(a, a)); }
+template <class R> inline R norm(V3<R> a) { return sqrt(dot(a, a)); }
 template <class R> inline V3<R> normalize(V3<R> a) { return a / norm(a); }
 // GLSL reflect / refract as taichi.math defines them
 template <class R> inline V3<R> reflect(V3<R> x, V3<R> n) { return x - (R(2) * dot(n, x)) * n; }
 template <class R> inline V3<R> refract(V3<R> x, V3<R> n, R eta) {
   const R dxn = dot(x, n);
   const R k = R(1) - eta * eta * (R(1) - dxn * dxn);
-  if (k >= R(0)) return eta * x - (eta * dxn + std::sqrt(k)) * n;
+  if (k >= R(0)) return eta * x - (eta * dxn + sqrt(k)) * n;
   return {R(0), R(0), R(0)};
 }
 template <class R> inline V3<R> load3(const float *p, int64_t i) {
   return {R(p[3 * i]), R(p[3 * i + 1]), R(p[3 * i + 2])};
 }
-template <class R> inline R clampr(R x, R lo, R hi) { return std::min(std::max(x, lo), hi); }
+template <class R> inline R clampr(R x, R lo, R hi) { return min(max(x, lo), hi); }
+template <class R> inline V3<R> detach3(V3<R> a) { return {detach(a.x), detach(a.y), detach(a.z)}; }
 
 constexpr double kPi = 3.14159265358979323846;
 
@@ -119,7 +219,26 @@ template <class R> struct Ctx {
   R absorb(R k, int band) const { return (four_pi * k) / (lmin_m + (R(band) * step) * R(1e-9)); }
   // the evaluate_bsdf form (main.py:1394): 4*pi*k*1e9 / lambda[nm]
   R absorb_nm(R k, int band) const { return (four_pi * k * R(1e9)) / (lmin_nm + R(band) * step); }
+  // adjoint oracle: derivative slot of each parameter (-1 = not selected),
+  // material table [M][6][B] then EEM [E][B][B]
+  const int32_t *slot = nullptr;
+  int64_t pmat = 0;
 };
+
+// A parameter value as the estimator reads it; the adjoint oracle seeds the
+// derivative of a selected parameter with 1.
+template <class R> inline R param(const Ctx<R> &x, float value, int64_t idx) {
+  R r(value);
+  if constexpr (is_dual<R>::value) {
+    if (x.slot) {
+      const int k = x.slot[idx];
+      if (k >= 0) r.d[k] = 1.0;
+    }
+  }
+  (void)x;
+  (void)idx;
+  return r;
+}
 
 template <class R> struct Mat {
   R n, k, rough, sigma_s, emission, g;
@@ -131,31 +250,33 @@ template <class R> inline Mat<R> get_mat(const Ctx<R> &x, int m, int band) {
   const float *f = x.s->mat_f32 + (int64_t)m * 6 * B;
   const int32_t *i = x.s->mat_i32 + (int64_t)m * 2 * B;
   Mat<R> r;
-  r.n = R(f[0 * B + band]);
-  r.k = R(f[1 * B + band]);
-  r.rough = R(f[2 * B + band]);
-  r.sigma_s = R(f[3 * B + band]);
-  r.emission = R(f[4 * B + band]);
-  r.g = R(f[5 * B + band]);
+  const int64_t base = (int64_t)m * 6 * B + band;
+  r.n = param(x, f[0 * B + band], base + 0 * B);
+  r.k = param(x, f[1 * B + band], base + 1 * B);
+  r.rough = param(x, f[2 * B + band], base + 2 * B);
+  r.sigma_s = param(x, f[3 * B + band], base + 3 * B);
+  r.emission = param(x, f[4 * B + band], base + 4 * B);
+  r.g = param(x, f[5 * B + band], base + 5 * B);
   r.is_vol = i[0 * B + band];
   r.surf_emis = i[1 * B + band];
   r.eem = x.s->mat_eem[m];
   return r;
 }
 template <class R> inline R eem_at(const Ctx<R> &x, int eem, int row, int col) {
-  return R(x.s->eem[((int64_t)eem * x.B + row) * x.B + col]);
+  const int64_t i = ((int64_t)eem * x.B + row) * x.B + col;
+  return param(x, x.s->eem[i], x.pmat + i);
 }
 
 // ---------------------------------------------------------------- sampling
 // random_in_unit_sphere, main.py:682-687
 template <class R> V3<R> random_in_unit_sphere(const Ctx<R> &x, Rng &rng) {
   const R z = R(rng.next()) * R(2) - R(1);
-  const R rxy = std::sqrt(std::max(R(0), R(1) - z * z));
+  const R rxy = sqrt(max(R(0), R(1) - z * z));
   const R phi = R(rng.next()) * R(2) * x.pi;
-  return {rxy * std::cos(phi), rxy * std::sin(phi), z};
+  return {rxy * cos(phi), rxy * sin(phi), z};
 }
 template <class R> inline void onb(V3<R> n, V3<R> &t, V3<R> &b) {
-  const V3<R> up = std::fabs(n.y) < R(0.999) ? mk<R>(0, 1, 0) : mk<R>(1, 0, 0);
+  const V3<R> up = fabs(n.y) < R(0.999) ? mk<R>(0, 1, 0) : mk<R>(1, 0, 0);
   t = normalize(cross(up, n));
   b = cross(n, t);
 }
@@ -164,32 +285,33 @@ template <class R> V3<R> cosine_hemisphere(const Ctx<R> &x, V3<R> n, Rng &rng) {
   const R r1 = R(rng.next());
   const R r2 = R(rng.next());
   const R phi = x.two_pi * r1;
-  const R ct = std::sqrt(R(1) - r2);
-  const R st = std::sqrt(r2);
+  const R ct = sqrt(R(1) - r2);
+  const R st = sqrt(r2);
   V3<R> t, b;
   onb(n, t, b);
-  return t * std::cos(phi) * st + b * std::sin(phi) * st + n * ct;
+  return t * cos(phi) * st + b * sin(phi) * st + n * ct;
 }
 // evaluate_henyey_greenstein, main.py:758-766
 template <class R> R hg_eval(const Ctx<R> &x, R cos_t, R g) {
   const R g2 = g * g;
   const R denom = R(1) + g2 - R(2) * g * cos_t;
-  return (R(1) - g2) / (x.four_pi * denom * std::sqrt(denom) + R(1e-6));
+  return (R(1) - g2) / (x.four_pi * denom * sqrt(denom) + R(1e-6));
 }
 // sample_henyey_greenstein, main.py:768-792
-template <class R> V3<R> hg_sample(const Ctx<R> &x, V3<R> w, R g, Rng &rng) {
+template <class R> V3<R> hg_sample(const Ctx<R> &x, V3<R> w, R g, Rng &rng, R *ct_out = nullptr) {
   R ct;
-  if (std::fabs(g) < R(1e-4)) {
+  if (fabs(g) < R(1e-4)) {
     ct = R(2) * R(rng.next()) - R(1);
   } else {
     const R rs = (R(1) - g * g) / (R(1) - g + R(2) * g * R(rng.next()));
     ct = (R(1) + g * g - rs * rs) / (R(2) * g);
   }
-  const R st = std::sqrt(std::max(R(0), R(1) - ct * ct));
+  if (ct_out) *ct_out = ct;
+  const R st = sqrt(max(R(0), R(1) - ct * ct));
   const R phi = x.two_pi * R(rng.next());
   V3<R> u, v;
   onb(w, u, v);
-  return u * std::cos(phi) * st + v * std::sin(phi) * st + w * ct;
+  return u * cos(phi) * st + v * sin(phi) * st + w * ct;
 }
 
 // ---------------------------------------------------------------- intersection
@@ -199,8 +321,8 @@ template <class R> inline bool hit_aabb(V3<R> o, V3<R> inv, V3<R> mn, V3<R> mx) 
   const R ax = (mn.x - o.x) * inv.x, bx = (mx.x - o.x) * inv.x;
   const R ay = (mn.y - o.y) * inv.y, by = (mx.y - o.y) * inv.y;
   const R az = (mn.z - o.z) * inv.z, bz = (mx.z - o.z) * inv.z;
-  const R te = std::fmax(std::fmin(ax, bx), std::fmax(std::fmin(ay, by), std::fmin(az, bz)));
-  const R tx = std::fmin(std::fmax(ax, bx), std::fmin(std::fmax(ay, by), std::fmax(az, bz)));
+  const R te = fmax(fmin(ax, bx), fmax(fmin(ay, by), fmin(az, bz)));
+  const R tx = fmin(fmax(ax, bx), fmin(fmax(ay, by), fmax(az, bz)));
   return te < tx && tx > R(0);
 }
 // intersect_triangle (Moller-Trumbore), main.py:807-829; returns t=-1 on miss
@@ -209,7 +331,7 @@ template <class R> inline void hit_tri(V3<R> o, V3<R> d, V3<R> v0, V3<R> e1, V3<
   t = R(-1); u = R(-1); v = R(-1);
   const V3<R> p = cross(d, e2);
   const R det = dot(e1, p);
-  if (std::fabs(det) > R(1e-8)) {
+  if (fabs(det) > R(1e-8)) {
     const R inv_det = R(1) / det;
     const V3<R> tv = o - v0;
     const R ut = dot(tv, p) * inv_det;
@@ -301,20 +423,20 @@ template <class R> inline C2<R> cdiv(C2<R> a, C2<R> b) {  // main.py:874-880
 }
 template <class R> inline R cmod2(C2<R> a) { return a.re * a.re + a.im * a.im; }
 template <class R> inline C2<R> csqrt(C2<R> z) {  // main.py:887-896
-  const R mod = std::sqrt(z.re * z.re + z.im * z.im);
-  const R re = std::sqrt((mod + z.re) / R(2));
+  const R mod = sqrt(z.re * z.re + z.im * z.im);
+  const R re = sqrt((mod + z.re) / R(2));
   const R sg = z.im > R(0) ? R(1) : (z.im < R(0) ? R(-1) : R(0));
-  R im = sg * std::sqrt((mod - z.re) / R(2));
+  R im = sg * sqrt((mod - z.re) / R(2));
   if (z.im == R(0)) im = R(0);
   return {re, im};
 }
 // fresnel_spectral, main.py:925-966
 template <class R> R fresnel(R cos_i, R ni, R ki, R nt, R kt) {
-  const R ang = std::acos(clampr(cos_i, R(-1), R(1)));
+  const R ang = acos(clampr(cos_i, R(-1), R(1)));
   const C2<R> e_in = {ni * ni - ki * ki, R(2) * ni * ki};
   const C2<R> e_tr = {nt * nt - kt * kt, R(2) * nt * kt};
-  const R ct = std::cos(ang);
-  const R s = std::sin(ang);
+  const R ct = cos(ang);
+  const R s = sin(ang);
   const R s2 = s * s;
   C2<R> left = cmul(csqrt(e_in), C2<R>{ct, R(0)});
   const C2<R> es = cmul(e_in, C2<R>{s2, R(0)});
@@ -336,12 +458,12 @@ template <class R> inline R ggx_d(const Ctx<R> &x, R ndh, R rough) {
 }
 // geometry_smith_ggx, main.py:909-923
 template <class R> inline R ggx_g(V3<R> n, V3<R> v, V3<R> l, R rough) {
-  const R ndv = std::max(dot(n, v), R(0));
+  const R ndv = max(dot(n, v), R(0));
   R a = rough * rough;
-  a = std::max(a, R(1e-4));
+  a = max(a, R(1e-4));
   const R k = a * a / R(2);
   const R gv = ndv / (ndv * (R(1) - k) + k + R(1e-7));
-  const R ndl = std::max(dot(n, l), R(0));
+  const R ndl = max(dot(n, l), R(0));
   const R gl = ndl / (ndl * (R(1) - k) + k + R(1e-7));
   return gv * gl;
 }
@@ -349,11 +471,11 @@ template <class R> inline R ggx_g(V3<R> n, V3<R> v, V3<R> l, R rough) {
 template <class R> V3<R> ggx_sample(const Ctx<R> &x, R xi0, R xi1, V3<R> n, R alpha) {
   const R a2 = alpha * alpha;
   const R phi = x.two_pi * xi0;
-  const R ct = std::sqrt((R(1) - xi1) / (R(1) + (a2 - R(1)) * xi1));
-  const R st = std::sqrt(R(1) - ct * ct);
+  const R ct = sqrt((R(1) - xi1) / (R(1) + (a2 - R(1)) * xi1));
+  const R st = sqrt(R(1) - ct * ct);
   V3<R> t, b;
   onb(n, t, b);
-  return normalize(t * (std::cos(phi) * st) + b * (std::sin(phi) * st) + n * ct);
+  return normalize(t * (cos(phi) * st) + b * (sin(phi) * st) + n * ct);
 }
 
 // ---------------------------------------------------------------- events
@@ -387,6 +509,11 @@ template <class R> inline R eem_row_max(const Ctx<R> &x, int eem, int row) {
   }
   return q;
 }
+template <class R> inline R eem_row_sum(const Ctx<R> &x, int eem, int row) {
+  R norm = R(0);
+  for (int j = 0; j < x.B; ++j) norm += eem_at(x, eem, row, j);
+  return norm;
+}
 template <class R> inline int eem_pick(const Ctx<R> &x, int eem, int row, R xi) {
   R norm = R(0);
   for (int j = 0; j < x.B; ++j) norm += eem_at(x, eem, row, j);
@@ -410,24 +537,42 @@ template <class R> SurfEvent<R> scatter_surface(const Ctx<R> &x, const Ray<R> &r
   const R ni = vm.n, ki = vm.k, nt = sm.n, kt = sm.k;
   const R xi0 = R(rng.next());
   const R xi1 = R(rng.next());
-  const V3<R> H = ggx_sample(x, xi0, xi1, N, sm.rough);
-  const R cin = std::max(R(1e-4), dot(V, H));
+  // the half vector is a sample: its density enters through its score
+  const V3<R> H = detach3(ggx_sample(x, xi0, xi1, N, sm.rough));
+  const R cin = max(R(1e-4), dot(V, H));
   const R F = fresnel(cin, ni, ki, nt, kt);
   const R pick = clampr(R(rng.next()), R(0), R(0.99));
+  R sc(1.0);  // product of the score factors of this event (adjoint oracle only)
+  if constexpr (is_dual<R>::value) {
+    if (sm.rough > R(0)) {
+      // sampler density a2 c / (pi (c^2 (a2 - 1) + 1)^2) with a2 = roughness^2; at the
+      // sampled c, c^2 = (1 - xi1) / (1 + (a2 - 1) xi1), so d log p / d roughness =
+      // (4 xi1 - 2) / roughness (the closed form avoids the cancellation near c = 1)
+      R s(1.0);
+      const auto k = (R(4) * xi1 - R(2)).v / sm.rough.v;
+      for (int i = 0; i < kDualN; ++i) s.d[i] = sm.rough.d[i] * k;
+      sc = sc * s;
+    }
+    if (pick < F) {
+      if (F <= R(0.99)) apply_score(sc, F);
+    } else {
+      apply_score(sc, R(1) - F);
+    }
+  }
   auto glossy_reflect = [&](bool abs_cos) {
     const V3<R> L = reflect(ray.dir, H);
     if (sm.rough < R(0.008)) {
       r.dir = L; r.did_reflect = 1; r.est = F; r.pdf = R(1e9);
     } else {
-      const R ndl = std::max(R(1e-4), dot(N, L));
-      const R ndh = std::max(R(1e-4), dot(N, H));
-      const R ndv = std::max(R(1e-4), dot(N, V));
+      const R ndl = max(R(1e-4), dot(N, L));
+      const R ndh = max(R(1e-4), dot(N, H));
+      const R ndv = max(R(1e-4), dot(N, V));
       const R D = ggx_d(x, ndh, sm.rough);
       const R G = ggx_g(N, V, L, sm.rough);
       const R bsdf = (D * G * F) / (R(4) * ndl * ndv);
       const R pdf = (D * ndh) / (R(4) * cin);
       r.dir = L; r.did_reflect = 1;
-      const R c = abs_cos ? std::fabs(dot(N, L)) : std::max(R(0), dot(N, L));
+      const R c = abs_cos ? fabs(dot(N, L)) : max(R(0), dot(N, L));
       r.est = (bsdf * c) / pdf;
       r.pdf = pdf;
     }
@@ -436,26 +581,27 @@ template <class R> SurfEvent<R> scatter_surface(const Ctx<R> &x, const Ray<R> &r
     glossy_reflect(false);
   } else {
     R absorb = x.absorb(kt, ray.active);
-    const R dist = -std::log(-R(rng.next()) + R(1) + R(1e-7)) / (sm.sigma_s + absorb + R(1e-6));
+    const R sig_t = sm.sigma_s + absorb + R(1e-6);
+    const R dist = detach(-log(-R(rng.next()) + R(1) + R(1e-7)) / sig_t);
     if (!sm.is_vol) {
       r.did_reflect = 1;
       const V3<R> S = cosine_hemisphere(x, N, rng);
-      const R ndl = std::max(R(1e-4), dot(N, S));
-      const R ndv = std::max(R(1e-4), dot(N, V));
+      const R ndl = max(R(1e-4), dot(N, S));
+      const R ndv = max(R(1e-4), dot(N, V));
       const R albedo = sm.sigma_s / (sm.sigma_s + absorb + R(1e-6));
       const R sigma = sm.rough * x.pi / R(2);
       const R s2 = sigma * sigma;
       const R A = R(1) - s2 / (R(2) * (s2 + R(0.33)));
       const R Bc = R(0.45) * s2 / (s2 + R(0.09));
-      const R th_i = std::acos(ndl), th_o = std::acos(ndv);
-      const R al = std::max(th_i, th_o), be = std::min(th_i, th_o);
+      const R th_i = acos(ndl), th_o = acos(ndv);
+      const R al = max(th_i, th_o), be = min(th_i, th_o);
       R cphi = R(0);
       if (ndl > R(1e-4) && ndv > R(1e-4)) {
         const V3<R> pi_ = normalize(S - N * ndl);
         const V3<R> po = normalize(V - N * ndv);
-        cphi = std::max(R(0), dot(pi_, po));
+        cphi = max(R(0), dot(pi_, po));
       }
-      R bsdf = (R(1) - F) * (albedo / x.pi) * (A + Bc * cphi * std::sin(al) * std::tan(be));
+      R bsdf = (R(1) - F) * (albedo / x.pi) * (A + Bc * cphi * sin(al) * tan(be));
       const R pdf = R(0.318309886184) * ndl;
       r.new_wl = ray.active;
       const int eem = sm.eem;
@@ -465,10 +611,15 @@ template <class R> SurfEvent<R> scatter_surface(const Ctx<R> &x, const Ray<R> &r
         if (qy > R(0) && xi3 < qy) {
           const R xi4 = R(rng.next());
           const int nw = eem_pick(x, eem, ray.active, xi4);
+          apply_score(sc, qy);
+          apply_score(sc, eem_at(x, eem, ray.active, nw) / eem_row_sum(x, eem, ray.active));
+          apply_score(sc, sig_t * exp(-sig_t * dist));  // the penetration distance is used now
           r.new_wl = nw;
           const Mat<R> smf = get_mat(x, ev.hit_mat, nw);
           absorb = x.absorb(smf.k, nw);
-          bsdf *= std::exp(-absorb * dist);
+          bsdf *= exp(-absorb * dist);
+        } else {
+          apply_score(sc, R(1) - qy);
         }
       }
       r.est = (bsdf * ndl) / pdf;
@@ -487,23 +638,24 @@ template <class R> SurfEvent<R> scatter_surface(const Ctx<R> &x, const Ray<R> &r
           r.pdf = R(1e9);
         } else {
           const R ldh = dot(T, H), vdh = dot(V, H);
-          const R ndh = std::max(R(1e-4), dot(N, H));
-          const R ndl = std::max(R(1e-4), std::fabs(dot(N, T)));
-          const R ndv = std::max(R(1e-4), std::fabs(dot(N, V)));
+          const R ndh = max(R(1e-4), dot(N, H));
+          const R ndl = max(R(1e-4), fabs(dot(N, T)));
+          const R ndv = max(R(1e-4), fabs(dot(N, V)));
           const R G = ggx_g(N, V, T, sm.rough);
           const R D = ggx_d(x, ndh, sm.rough);
           const R den = ni * vdh + nt * ldh;
           const R den2 = den * den;
-          const R t1 = std::fabs(ldh * vdh) / (ndl * ndv);
+          const R t1 = fabs(ldh * vdh) / (ndl * ndv);
           const R t2 = (nt * nt * (R(1) - F) * D * G) / den2;
           const R bsdf = t1 * t2;
-          const R pdf = (D * ndh * (R(1) - F) * nt * nt * std::fabs(ldh)) / den2;
+          const R pdf = (D * ndh * (R(1) - F) * nt * nt * fabs(ldh)) / den2;
           r.est = (bsdf * ndl) / pdf;
           r.pdf = pdf;
         }
       }
     }
   }
+  if constexpr (is_dual<R>::value) r.est = r.est * sc;
   return r;
 }
 
@@ -516,7 +668,9 @@ template <class R> VolEvent<R> scatter_volume(const Ctx<R> &x, const Ray<R> &ray
   r.dir = ray.dir;
   r.pen = ray.pen;
   const R absorb = x.absorb(vm.k, ray.active);
-  const R dvol = -std::log(-R(rng.next()) + R(1) - R(1e-7)) / (vm.sigma_s + absorb + R(1e-6));
+  const R sig_t = vm.sigma_s + absorb + R(1e-6);
+  // the free-flight distance is a sample: its density enters through its score
+  const R dvol = detach(-log(-R(rng.next()) + R(1) - R(1e-7)) / sig_t);
   st->traces++;
   const Hit<R> hit = trace(x, ray.pos, ray.dir, &st->stack_overflow);
   const R dsurf = hit.t;
@@ -531,7 +685,7 @@ template <class R> VolEvent<R> scatter_volume(const Ctx<R> &x, const Ray<R> &ray
   const R f = R(hit.front);
   r.normal = hit.normal * f - hit.normal * (R(1) - f);
   r.snormal = hit.shading_normal * f - hit.shading_normal * (R(1) - f);
-  const R T = std::exp(-(absorb + vm.sigma_s) * travel);
+  const R T = exp(-(absorb + vm.sigma_s) * travel);
   const R emit = ((-T + R(1)) * vm.emission) / (absorb + R(1e-6));
   const R att = T + emit;
   if (travel == dsurf) {
@@ -539,6 +693,8 @@ template <class R> VolEvent<R> scatter_volume(const Ctx<R> &x, const Ray<R> &ray
     r.action = 1;
     r.hit_mat = hit.mat;
     r.tri = hit.tri;
+    // P(free flight >= d_surf - eps)
+    apply_score(r.est, exp(-sig_t * detach(max(R(0), dsurf - x.eps))));
   } else if (travel >= R(0)) {
     r.hit_mat = -1;
     r.tri = -1;
@@ -556,17 +712,30 @@ template <class R> VolEvent<R> scatter_volume(const Ctx<R> &x, const Ray<R> &ray
           r.dir = random_in_unit_sphere(x, rng);
           const R em2 = ((-(R(1) - T) + R(1)) * get_mat(x, ray.vol, nw).emission) / (absorb + R(1e-6));
           r.est = (R(1) - T) + em2;
+          apply_score(r.est, qy);
+          apply_score(r.est, eem_at(x, vm.eem, ray.active, nw) / eem_row_sum(x, vm.eem, ray.active));
         } else {
           r.est = att;
+          apply_score(r.est, R(1) - qy);
         }
       } else {
         r.est = att / (R(1) + R(1e-6));
       }
+      apply_score(r.est, kind);
     } else {
       r.action = 2;
-      r.dir = hg_sample(x, ray.dir, vm.g, rng);
+      R ct(0.0);
+      r.dir = detach3(hg_sample(x, ray.dir, vm.g, rng, &ct));
       r.est = att;
+      apply_score(r.est, R(1) - kind);
+      if (fabs(vm.g) >= R(1e-4)) {  // the HG density the sampler draws from (no 1e-6 term)
+        const R g2 = vm.g * vm.g;
+        const R c = detach(ct);
+        const R den = R(1) + g2 - R(2) * vm.g * c;
+        apply_score(r.est, (R(1) - g2) / (x.four_pi * den * sqrt(den)));
+      }
     }
+    apply_score(r.est, sig_t * exp(-sig_t * travel));  // free-flight density at the event
   }
   return r;
 }
@@ -577,18 +746,18 @@ template <class R> void evaluate_bsdf(const Ctx<R> &x, int vol, int surf, V3<R> 
   const Mat<R> vm = get_mat(x, vol, wl);
   const Mat<R> sm = get_mat(x, surf, wl);
   const R ni = vm.n, ki = vm.k, nt = sm.n, kt = sm.k;
-  const R ndl = std::max(R(1e-4), dot(N, L));
-  const R ndv = std::max(R(1e-4), dot(N, V));
+  const R ndl = max(R(1e-4), dot(N, L));
+  const R ndv = max(R(1e-4), dot(N, V));
   const bool reflected = ndv * ndl > R(0);
   bsdf = R(0);
   pdf = R(0);
   if (reflected) {
     V3<R> H = normalize(V + L);
     if (dot(H, N) < R(0)) H = -H;
-    const R vdh = std::max(R(1e-4), dot(V, H));
+    const R vdh = max(R(1e-4), dot(V, H));
     const R F = fresnel(vdh, ni, ki, nt, kt);
     if (sm.rough > R(0.008)) {
-      const R ndh = std::max(R(1e-4), dot(N, H));
+      const R ndh = max(R(1e-4), dot(N, H));
       const R D = ggx_d(x, ndh, sm.rough);
       const R G = ggx_g(N, V, L, sm.rough);
       bsdf += (D * G * F) / (R(4) * ndl * ndv);
@@ -600,31 +769,31 @@ template <class R> void evaluate_bsdf(const Ctx<R> &x, int vol, int surf, V3<R> 
     const R s2 = sigma * sigma;
     const R A = R(1) - s2 / (R(2) * (s2 + R(0.33)));
     const R Bc = R(0.45) * s2 / (s2 + R(0.09));
-    const R th_i = std::acos(ndl), th_o = std::acos(ndv);
-    const R al = std::max(th_i, th_o), be = std::min(th_i, th_o);
+    const R th_i = acos(ndl), th_o = acos(ndv);
+    const R al = max(th_i, th_o), be = min(th_i, th_o);
     R cphi = R(0);
     if (ndl > R(1e-4) && ndv > R(1e-4)) {
       const V3<R> pi_ = normalize(L - N * ndl);
       const V3<R> po = normalize(V - N * ndv);
-      cphi = std::max(R(0), dot(pi_, po));
+      cphi = max(R(0), dot(pi_, po));
     }
     const R nv = R(1) - R(sm.is_vol);
-    bsdf += (R(1) - F) * nv * (albedo / x.pi) * (A + Bc * cphi * std::sin(al) * std::tan(be));
+    bsdf += (R(1) - F) * nv * (albedo / x.pi) * (A + Bc * cphi * sin(al) * tan(be));
     pdf += ndl * R(0.318309886184) * (R(1) - F) * nv;
   } else if (sm.rough > R(0.008)) {
     // transmission lobe; unreachable because both cosines are clamped to >= 1e-4
     V3<R> H = -normalize(V * ni + L * nt);
     if (dot(H, N) < R(0)) H = -H;
     const R vdh = dot(V, H), ldh = dot(L, H);
-    const R ndh = std::max(R(1e-4), dot(N, H));
+    const R ndh = max(R(1e-4), dot(N, H));
     if (vdh * ldh < R(0)) {
-      const R F = fresnel(std::fabs(vdh), ni, ki, nt, kt);
+      const R F = fresnel(fabs(vdh), ni, ki, nt, kt);
       const R D = ggx_d(x, ndh, sm.rough);
       const R G = ggx_g(N, V, L, sm.rough);
       const R den = ni * vdh + nt * ldh;
       const R den2 = den * den;
-      bsdf += (std::fabs(ldh * vdh) / std::fabs(ndl * ndv)) * ((nt * nt * (R(1) - F) * D * G) / den2);
-      pdf += (D * ndh * (R(1) - F) * nt * nt * std::fabs(ldh)) / den2;
+      bsdf += (fabs(ldh * vdh) / fabs(ndl * ndv)) * ((nt * nt * (R(1) - F) * D * G) / den2);
+      pdf += (D * ndh * (R(1) - F) * nt * nt * fabs(ldh)) / den2;
     }
   }
 }
@@ -644,9 +813,9 @@ template <class R> R shadow_transmittance(const Ctx<R> &x, V3<R> origin, V3<R> d
     const R dsurf = hit.t;
     const Mat<R> vm = get_mat(x, cur_vol, wl);
     const R absorb = x.absorb(vm.k, wl);
-    total *= std::exp(-(absorb + vm.sigma_s) * hit.t);
+    total *= exp(-(absorb + vm.sigma_s) * hit.t);
     if (hit.t >= (max_dist - traveled) || hit.tri == light_tri) {
-      total *= std::exp(-(absorb + vm.sigma_s) * (max_dist - traveled));
+      total *= exp(-(absorb + vm.sigma_s) * (max_dist - traveled));
       break;
     }
     const Mat<R> sm = get_mat(x, hit.mat, wl);
@@ -700,30 +869,47 @@ template <class R> Nee<R> sample_direct_light(const Ctx<R> &x, const Ray<R> &ray
   if (T > R(1e-6)) {
     const int lmat = s->mat_id[lt];
     const V3<R> ln = load3<R>(s->normal, lt);
-    const R cosl = std::max(R(0), dot(ln, -Ldir));
+    const R cosl = max(R(0), dot(ln, -Ldir));
     const R dsq = dist * dist;
     const R G = cosl / (dsq + R(1e-4));
     R bsdf, pdf, c;
     if (surf != -1) {
-      c = std::max(R(0), dot(N, Ldir));
+      c = max(R(0), dot(N, Ldir));
       evaluate_bsdf(x, ray.vol, surf, -ray.dir, Ldir, N, wl, bsdf, pdf);
     } else {
-      c = std::max(R(0), dot(ray.dir, Ldir));
+      c = max(R(0), dot(ray.dir, Ldir));
       bsdf = hg_eval(x, c, get_mat(x, ray.vol, wl).g);
       pdf = bsdf;
     }
     const R area = R(s->light_area[wl]);
     r.factor = bsdf * c * T * G * area;
     r.emission = get_mat(x, lmat, ray.transport).emission;
-    const R pl = dsq / (std::max(R(1e-6), cosl) * area);
+    const R pl = dsq / (max(R(1e-6), cosl) * area);
     r.weight = (pl * pl) / (pl * pl + pdf * pdf + R(1e-6));
   }
   return r;
 }
 
 // cast_rays body for one pixel, main.py:1502-1590
-template <class R> void render_pixel(const Ctx<R> &x, uint32_t pass, int band, int pid, double *acc,
-                                     orc_stats *st) {
+// Film deposit of the plain estimators: the value into the pixel's band.
+struct FilmSink {
+  double *acc;
+  template <class R> void operator()(int band, const R &v) { acc[band] += double(v); }
+};
+// Adjoint oracle: the value into the film (if any) and w[band] * d value into grad.
+struct GradSink {
+  double *acc;
+  const double *w;
+  double *grad;
+  int n;
+  template <class R> void operator()(int band, const R &v) {
+    if (acc) acc[band] += double(v.v);
+    for (int i = 0; i < n; ++i) grad[i] += w[band] * double(v.d[i]);
+  }
+};
+
+template <class R, class Sink> void render_pixel(const Ctx<R> &x, uint32_t pass, int band, int pid, Sink &sink,
+                                                 orc_stats *st) {
   const orc_config *c = x.c;
   const orc_scene *s = x.s;
   const int W = c->width, Hh = c->height;
@@ -764,8 +950,8 @@ template <class R> void render_pixel(const Ctx<R> &x, uint32_t pass, int band, i
       const Mat<R> sm = get_mat(x, ev.hit_mat, ray.transport);
       if (sm.surf_emis) {
         const R dsq = ev.travel * ev.travel;
-        const R cosl = std::max(R(0), dot(load3<R>(s->normal, ev.tri), -ray.dir));
-        const R pl = (dsq * std::min(R(1), R(ray.plen))) /
+        const R cosl = max(R(0), dot(load3<R>(s->normal, ev.tri), -ray.dir));
+        const R pl = (dsq * min(R(1), R(ray.plen))) /
                      (cosl * R(s->light_area[ray.active]) + R(1e-6));
         const R w = (ray.spdf * ray.spdf) / (pl * pl + ray.spdf * ray.spdf + R(1e-6));
         indirect = ray.thr * sm.emission * w;
@@ -796,8 +982,8 @@ template <class R> void render_pixel(const Ctx<R> &x, uint32_t pass, int band, i
         ray.plen++;
       }
     }
-    acc[active_px] += double(indirect);
-    acc[active_px] += double(direct);
+    sink(active_px, indirect);
+    sink(active_px, direct);
     // A path whose throughput is exactly zero can only deposit zeros from
     // here on -- or NaN, where a later degenerate event computes 0/0 (the
     // rough-dielectric exit of an index-matched interface does).  Such paths
@@ -820,7 +1006,10 @@ void render_pass_t(const orc_scene *s, const orc_config *c, uint32_t pass, int b
 #ifdef _OPENMP
 #pragma omp for schedule(dynamic, 16)
 #endif
-    for (int p = 0; p < npix; ++p) render_pixel(x, pass, band, pix[p], out + (int64_t)p * c->bands, &st);
+    for (int p = 0; p < npix; ++p) {
+      FilmSink sink{out + (int64_t)p * c->bands};
+      render_pixel(x, pass, band, pix[p], sink, &st);
+    }
 #ifdef _OPENMP
 #pragma omp critical
 #endif
@@ -832,6 +1021,46 @@ void render_pass_t(const orc_scene *s, const orc_config *c, uint32_t pass, int b
     }
   }
   if (stats) *stats = tot;
+}
+
+// Forward-mode adjoint of one pass for up to kDualN parameters at a time.
+template <class T>
+void adjoint_pass_t(const orc_scene *s, const orc_config *c, uint32_t pass, int band, const int32_t *pix, int npix,
+                    const double *adj, int nparams, const int64_t *ids, double *grad, double *out, int nthreads) {
+  using DR = Dual<T, kDualN>;
+  const int B = c->bands;
+  const int64_t pmat = (int64_t)s->num_materials * 6 * B;
+  const int64_t ptot = pmat + (int64_t)s->num_eems * B * B;
+  std::vector<int32_t> slot(ptot, -1);
+  for (int p0 = 0; p0 < nparams; p0 += kDualN) {
+    const int n = std::min(kDualN, nparams - p0);
+    std::fill(slot.begin(), slot.end(), -1);
+    for (int i = 0; i < n; ++i)
+      if (ids[p0 + i] >= 0 && ids[p0 + i] < ptot) slot[ids[p0 + i]] = i;
+    Ctx<DR> x(s, c);
+    x.slot = slot.data();
+    x.pmat = pmat;
+    double *film = p0 == 0 ? out : nullptr;
+#ifdef _OPENMP
+    const int nt = nthreads > 0 ? nthreads : omp_get_max_threads();
+#pragma omp parallel num_threads(nt)
+#endif
+    {
+      std::vector<double> g(n, 0.0);
+      orc_stats st{0, 0, 0, 0};
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 16)
+#endif
+      for (int p = 0; p < npix; ++p) {
+        GradSink sink{film ? film + (int64_t)p * B : nullptr, adj + (int64_t)p * B, g.data(), n};
+        render_pixel(x, pass, band, pix[p], sink, &st);
+      }
+#ifdef _OPENMP
+#pragma omp critical
+#endif
+      for (int i = 0; i < n; ++i) grad[p0 + i] += g[i];
+    }
+  }
 }
 
 // ---------------------------------------------------------------- BVH sweep builder
@@ -1007,6 +1236,15 @@ void orc_render_pass(const orc_scene *s, const orc_config *c, uint32_t pass_idx,
     render_pass_t<double>(s, c, pass_idx, band, pixel_ids, npix, out, nthreads, stats);
   else
     render_pass_t<float>(s, c, pass_idx, band, pixel_ids, npix, out, nthreads, stats);
+}
+
+void orc_adjoint_pass(const orc_scene *s, const orc_config *c, uint32_t pass_idx, int32_t band,
+                      const int32_t *pixel_ids, int32_t npix, const double *adj, int32_t nparams,
+                      const int64_t *param_ids, double *grad, double *out, int32_t use_double, int32_t nthreads) {
+  if (use_double)
+    adjoint_pass_t<double>(s, c, pass_idx, band, pixel_ids, npix, adj, nparams, param_ids, grad, out, nthreads);
+  else
+    adjoint_pass_t<float>(s, c, pass_idx, band, pixel_ids, npix, adj, nparams, param_ids, grad, out, nthreads);
 }
 
 int32_t orc_build_bvh_sweep(int32_t num_tris, const float *v0, const float *v1, const float *v2,

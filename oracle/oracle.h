@@ -97,6 +97,17 @@ void orc_render_pass(const orc_scene *s, const orc_config *c, uint32_t pass_idx,
                      const int32_t *pixel_ids, int32_t npix, double *out, int32_t use_double,
                      int32_t nthreads, orc_stats *stats);
 
+/* Forward-mode adjoint of one pass, in FP64 or FP32 (forward-mode dual numbers
+ * through the same estimator, sampled values held fixed and every
+ * parameter-dependent sampling decision multiplied by its score factor p/p).
+ * param_ids index the material table [M][6][B] followed by the EEM table
+ * [E][B][B].  adj: [npix][B] weights of the film deposits.  ADDS
+ * sum_p sum_b adj[p][b] * d deposit[p][b] / d param into grad[nparams];
+ * out (may be NULL) receives the film of the pass like orc_render_pass. */
+void orc_adjoint_pass(const orc_scene *s, const orc_config *c, uint32_t pass_idx, int32_t band,
+                      const int32_t *pixel_ids, int32_t npix, const double *adj, int32_t nparams,
+                      const int64_t *param_ids, double *grad, double *out, int32_t use_double, int32_t nthreads);
+
 /* The reference SAH builder (build_bvh, main.py:437-507): full sweep over all
  * split positions on 3 axes, leaf at <=10 triangles or when no split beats
  * the leaf cost, flat boxes padded by 1e-6, depth-first node order.  Centroid

@@ -66,6 +66,11 @@ def lib():
         L.orc_render_pass.argtypes = [ctypes.POINTER(OrcScene), ctypes.POINTER(OrcConfig), ctypes.c_uint32,
                                       ctypes.c_int32, I32P, ctypes.c_int32, ctypes.POINTER(ctypes.c_double),
                                       ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(OrcStats)]
+        L.orc_adjoint_pass.argtypes = [ctypes.POINTER(OrcScene), ctypes.POINTER(OrcConfig), ctypes.c_uint32,
+                                       ctypes.c_int32, I32P, ctypes.c_int32, ctypes.POINTER(ctypes.c_double),
+                                       ctypes.c_int32, ctypes.POINTER(ctypes.c_int64),
+                                       ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                       ctypes.c_int32, ctypes.c_int32]
         L.orc_build_bvh_sweep.argtypes = [ctypes.c_int32, F32P, F32P, F32P, ctypes.c_int32, F32P, F32P,
                                           I32P, I32P, I32P, I32P, I32P]
         L.orc_build_bvh_sweep.restype = ctypes.c_int32
@@ -194,6 +199,40 @@ def render_pass(scene, cfg, pass_idx, band, pixel_ids, out=None, use_double=Fals
                           ctypes.byref(st))
     return out, {"paths": st.paths, "vertices": st.vertices, "traces": st.traces,
                  "stack_overflow": st.stack_overflow}
+
+
+def adjoint_pass(scene, cfg, pass_idx, band, pixel_ids, adj, param_ids, grad=None, out=None, use_double=True,
+                 nthreads=0):
+    """Forward-mode adjoint of one pass (FP64, or FP32 with use_double=False): ADDS d(sum adj * deposits)/d params into grad.
+
+    adj: [npix, B] float64 deposit weights; param_ids: indices into the
+    material table [M,6,B] followed by the EEM table [E,B,B].  out (optional,
+    [npix, B] float64) receives the pass's FP64 film."""
+    pixel_ids = _i32(pixel_ids)
+    npix = pixel_ids.shape[0]
+    adj = np.ascontiguousarray(adj, np.float64)
+    assert adj.shape == (npix, cfg.c.bands)
+    ids = np.ascontiguousarray(param_ids, np.int64)
+    if grad is None:
+        grad = np.zeros(ids.shape[0], np.float64)
+    assert grad.dtype == np.float64 and grad.shape == ids.shape
+    dp = ctypes.POINTER(ctypes.c_double)
+    outp = None if out is None else out.ctypes.data_as(dp)
+    if out is not None:
+        assert out.dtype == np.float64 and out.flags.c_contiguous and out.shape == (npix, cfg.c.bands)
+    lib().orc_adjoint_pass(ctypes.byref(scene.s), ctypes.byref(cfg.c), pass_idx, band, _p(pixel_ids, I32P), npix,
+                           adj.ctypes.data_as(dp), ids.shape[0], ids.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                           grad.ctypes.data_as(dp), outp, int(use_double), nthreads)
+    return grad
+
+
+def param_index(num_materials, bands, material, prop, band):
+    """Index of material-table entry (material, prop, band) in the parameter vector."""
+    return (material * 6 + prop) * bands + band
+
+
+def eem_param_index(num_materials, bands, eem, row, col):
+    return num_materials * 6 * bands + (eem * bands + row) * bands + col
 
 
 def build_bvh_sweep(v0, v1, v2):

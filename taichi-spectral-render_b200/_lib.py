@@ -87,6 +87,9 @@ SIGNATURES = [
                                       ctypes.c_int32, _VP, _VP]),
     ("ts_trace_batch", ctypes.c_int, [_VP, _VP, ctypes.c_int32, ctypes.c_int32, _VP, _VP, _VP, _VP, _VP]),
     ("ts_render_normals", ctypes.c_int, [_VP, _VP, _VP]),
+    ("ts_param_count", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]),
+    ("ts_update_materials", ctypes.c_int, [_VP, _VP, _VP, _VP]),
+    ("ts_adjoint_pass", ctypes.c_int, [_VP, ctypes.c_uint32, ctypes.c_int32, _VP, _VP, _VP]),
     ("ts_check_device", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_uint32)]),
 ]
 

@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "bvh.h"
+#include "adjoint.cuh"
 #include "kernels.cuh"
 #include "spectral.h"
 
@@ -37,6 +38,8 @@ struct ts_ctx {
   uint32_t *d_err = nullptr;
   float *d_xyz = nullptr;
   float *d_m9 = nullptr;  // XYZ->RGB matrix for ts_resolve_rgb
+  float4 *d_mat = nullptr;  // packed material table (scene allocation), rewritten by ts_update_materials
+  float *d_eem = nullptr, *d_qy = nullptr, *d_cdf = nullptr;
   ts::WaveBuffers wave{};
   std::vector<void *> wave_allocs;
   size_t film_bytes = 0, scene_bytes = 0, wave_bytes = 0;
@@ -358,6 +361,10 @@ ts_status ts_upload_scene(ts_ctx *c, const ts_scene_desc *sd) {
   ds.ref_link = d_rlink;
   ds.num_ref_nodes = (int)bvh.ref_link.size();
   ds.mat = d_mat;
+  c->d_mat = d_mat;
+  c->d_eem = d_eem;
+  c->d_qy = d_qy;
+  c->d_cdf = d_cdf;
   ds.mat_eem = d_meem;
   ds.eem = d_eem;
   ds.eem_qy = d_qy;
@@ -602,6 +609,44 @@ ts_status ts_render_normals(ts_ctx *c, float *out, void *stream) {
   if (!c->has_scene) return fail(c, TS_ERR_NO_SCENE, "ts_render_normals: no scene uploaded");
   cudaSetDevice(c->cfg.device);
   TS_CUDA(c, ts::launch_render_normals(c->ds, c->dc, out, c->d_err, as_stream(stream)), "render normals");
+  return TS_OK;
+}
+
+ts_status ts_param_count(const ts_ctx *c, int64_t *num_material_params, int64_t *num_eem_params) {
+  if (!c || !num_material_params || !num_eem_params)
+    return fail(nullptr, TS_ERR_INVALID_ARG, "ts_param_count: null argument");
+  if (!c->has_scene) return fail(const_cast<ts_ctx *>(c), TS_ERR_NO_SCENE, "ts_param_count: no scene uploaded");
+  const int64_t B = c->cfg.bands;
+  *num_material_params = (int64_t)c->ds.num_materials * 6 * B;
+  *num_eem_params = (int64_t)c->ds.num_eems * B * B;
+  return TS_OK;
+}
+
+ts_status ts_update_materials(ts_ctx *c, const float *mat_f32_dev, const float *eem_dev, void *stream) {
+  if (!c) return fail(nullptr, TS_ERR_INVALID_ARG, "ts_update_materials: null context");
+  if (!c->has_scene) return fail(c, TS_ERR_NO_SCENE, "ts_update_materials: no scene uploaded");
+  if (eem_dev && c->ds.num_eems <= 0)
+    return fail(c, TS_ERR_INVALID_ARG, "ts_update_materials: the scene has no EEM table");
+  cudaSetDevice(c->cfg.device);
+  TS_CUDA(c, ts::launch_update_materials(c->d_mat, mat_f32_dev, c->ds.num_materials, c->cfg.bands, c->d_eem, c->d_qy,
+                                         c->d_cdf, eem_dev, c->ds.num_eems, as_stream(stream)),
+          "ts_update_materials");
+  return TS_OK;
+}
+
+ts_status ts_adjoint_pass(ts_ctx *c, uint32_t pass_idx, int32_t band, const double *adj_dev, double *grad_dev,
+                          void *stream) {
+  if (!c || !adj_dev || !grad_dev) return fail(c, TS_ERR_INVALID_ARG, "ts_adjoint_pass: null argument");
+  if (!c->has_scene) return fail(c, TS_ERR_NO_SCENE, "ts_adjoint_pass: no scene uploaded");
+  if (band < 0 || band >= c->cfg.bands) return fail(c, TS_ERR_INVALID_ARG, "ts_adjoint_pass: band out of range");
+  if (c->cfg.scatter_bounces > ts::kAdjMaxSeg)
+    return fail(c, TS_ERR_INVALID_ARG, "ts_adjoint_pass: scatter_bounces above " + std::to_string(ts::kAdjMaxSeg) +
+                                           " is not supported by the adjoint");
+  cudaSetDevice(c->cfg.device);
+  const int grid = c->num_sms * 4;
+  TS_CUDA(c, ts::launch_adjoint(c->ds, c->dc, pass_idx, band, adj_dev, grad_dev, c->d_counter, c->d_err, grid,
+                                as_stream(stream)),
+          "ts_adjoint_pass");
   return TS_OK;
 }
 

@@ -80,7 +80,7 @@ TS_D float hg_eval(float cos_t, float g) {  // main.py:758-766
   return (1.0f - g2) / (kFourPiF * denom * sqrtf(denom) + 1e-6f);
 }
 
-TS_D float3 hg_sample(float3 w, float g, Rng &rng) {  // main.py:768-792
+TS_D float3 hg_sample(float3 w, float g, Rng &rng, float *ct_out = nullptr) {  // main.py:768-792
   float ct;
   if (fabsf(g) < 1e-4f) {
     ct = 2.0f * rng.next() - 1.0f;
@@ -88,6 +88,7 @@ TS_D float3 hg_sample(float3 w, float g, Rng &rng) {  // main.py:768-792
     const float rs = (1.0f - g * g) / (1.0f - g + 2.0f * g * rng.next());
     ct = (1.0f + g * g - rs * rs) / (2.0f * g);
   }
+  if (ct_out) *ct_out = ct;
   const float st = sqrtf(fmaxf(0.f, 1.0f - ct * ct));
   const float phi = kTwoPiF * rng.next();
   float3 u, v;
@@ -201,6 +202,8 @@ struct VolEvent {
   float travel, est;
   float3 normal, snormal, dir;
   int front, hit_mat, tri, new_wl;
+  float dsurf;   // distance to the closest surface (1e9 on a miss)
+  float hg_ct;   // sampled phase cosine of a scattering event
 };
 
 TS_D float eem_cdf_pick(const DevScene &s, int B, int eem, int row, float xi) {
@@ -232,6 +235,8 @@ TS_D VolEvent volume_event(const DevScene &s, const DevConfig &c, const PathStat
     if (dvol + c.eps < travel) travel = dvol;
   }
   r.travel = travel;
+  r.dsurf = dsurf;
+  r.hg_ct = 1.f;
   SurfaceInfo si;
   if (hit.slot >= 0) {
     si = surface_info(s, hit, p.dir);
@@ -275,7 +280,7 @@ TS_D VolEvent volume_event(const DevScene &s, const DevConfig &c, const PathStat
       }
     } else {
       r.action = 2;
-      r.dir = hg_sample(p.dir, vm.g, rng);
+      r.dir = hg_sample(p.dir, vm.g, rng, &r.hg_ct);
       r.est = att;
     }
   }
@@ -318,6 +323,9 @@ struct ShadowQuery {
   float max_dist;
   int light_slot, vol, band;
   float contrib;  // everything of the direct term except the transmittance
+  // factors of contrib, kept for the adjoint: contrib = thr * em * bsdf * cs * ga * weight
+  float em, bsdf, pdf, cs, ga, pl;
+  int lmat;
 };
 
 // sample_direct_light up to the shadow test (main.py:1296-1358).  Returns
@@ -372,6 +380,13 @@ TS_D bool nee_setup(const DevScene &s, const DevConfig &c, const PathState &p, i
   const float pl = dsq / (fmaxf(1e-6f, cosl) * area);
   const float weight = (pl * pl) / (pl * pl + pdf * pdf + 1e-6f);
   q.contrib = p.thr * emission * (bsdf * cs * G * area) * weight;
+  q.em = emission;
+  q.bsdf = bsdf;
+  q.pdf = pdf;
+  q.cs = cs;
+  q.ga = G * area;
+  q.pl = pl;
+  q.lmat = lmat;
   return true;
 }
 
@@ -428,7 +443,15 @@ struct SurfEvent {
   int did_reflect;
   float3 dir;
   float est, pdf;
+  // sampling record, kept for the adjoint
+  float3 H;      // sampled GGX half vector
+  float xi1;     // its polar random number (the sampler's density follows from it exactly)
+  float F, cin;  // Fresnel term at cin = max(1e-4, V.H)
+  float dist;    // penetration distance (used by surface fluorescence)
+  int branch;    // kSurfGlossy, kSurfDiffuse, kSurfTransmit, kSurfTir
+  int fl;        // surface fluorescence: -1 no test, -2 rejected, >= 0 accepted band
 };
+enum { kSurfGlossy = 0, kSurfDiffuse = 1, kSurfTransmit = 2, kSurfTir = 3 };
 
 // scatter_surface, main.py:1000-1188
 TS_D SurfEvent scatter_surface(const DevScene &s, const DevConfig &c, const PathState &p, const VolEvent &ev,
@@ -448,13 +471,22 @@ TS_D SurfEvent scatter_surface(const DevScene &s, const DevConfig &c, const Path
   const float cin = fmaxf(1e-4f, dot(V, H));
   const float F = fresnel(cin, vm.n, vm.k, sm.n, sm.k);
   const float pick = fminf(fmaxf(rng.next(), 0.f), 0.99f);
+  r.H = H;
+  r.xi1 = xi1;
+  r.F = F;
+  r.cin = cin;
+  r.dist = 0.f;
+  r.fl = -1;
+  r.branch = kSurfGlossy;
   bool glossy = false, abs_cos = false;
   if (pick < F) {
     glossy = true;
   } else {
     const float absorb = absorb_m(c, sm.k, p.active);
     const float dist = -logf(-rng.next() + 1.0f + 1e-7f) / (sm.sigma_s + absorb + 1e-6f);
+    r.dist = dist;
     if (!sm.is_vol) {
+      r.branch = kSurfDiffuse;
       r.did_reflect = 1;
       const float3 S = cosine_hemisphere(N, rng);
       const float ndl = fmaxf(1e-4f, dot(N, S));
@@ -467,8 +499,10 @@ TS_D SurfEvent scatter_surface(const DevScene &s, const DevConfig &c, const Path
       if (sm.eem > 0) {
         const float qy = __ldg(s.eem_qy + (size_t)sm.eem * c.B + p.active);
         const float xi3 = rng.next();
+        r.fl = -2;
         if (qy > 0.f && xi3 < qy) {
           const int nw = (int)eem_cdf_pick(s, c.B, sm.eem, p.active, rng.next());
+          r.fl = nw;
           const Mat smf = get_mat(s, c.B, ev.hit_mat, nw);
           bsdf *= expf(-absorb_m(c, smf.k, nw) * dist);
         }
@@ -481,7 +515,9 @@ TS_D SurfEvent scatter_surface(const DevScene &s, const DevConfig &c, const Path
       if (dot(T, T) < 1e-4f) {
         glossy = true;
         abs_cos = true;
+        r.branch = kSurfTir;
       } else {
+        r.branch = kSurfTransmit;
         r.did_reflect = 0;
         r.dir = T;
         if (sm.rough < 0.0018f) {
@@ -529,7 +565,7 @@ TS_D SurfEvent scatter_surface(const DevScene &s, const DevConfig &c, const Path
 
 // Direct hit on an emitter (main.py:1548-1559)
 TS_D float emitter_hit(const DevScene &s, const DevConfig &c, const PathState &p, const VolEvent &ev,
-                       float emission) {
+                       float emission, float *w_out = nullptr, float *pl_out = nullptr) {
   const float4 s0 = __ldg(s.shade + 3 * (size_t)ev.tri + 0);
   const float4 s1 = __ldg(s.shade + 3 * (size_t)ev.tri + 1);
   const float4 s2 = __ldg(s.shade + 3 * (size_t)ev.tri + 2);
@@ -538,6 +574,8 @@ TS_D float emitter_hit(const DevScene &s, const DevConfig &c, const PathState &p
   const float cosl = fmaxf(0.f, dot(ln, -p.dir));
   const float pl = (dsq * fminf(1.0f, (float)p.plen)) / (cosl * __ldg(s.light_area + p.active) + 1e-6f);
   const float w = (p.spdf * p.spdf) / (pl * pl + p.spdf * p.spdf + 1e-6f);
+  if (w_out) *w_out = w;
+  if (pl_out) *pl_out = pl;
   return p.thr * emission * w;
 }
 

@@ -60,6 +60,16 @@ cudaError_t launch_wave_pass(const DevScene &s, const DevConfig &c, uint32_t pas
                              const WaveBuffers &w, uint32_t *err, int grid, int block, int sort_keys,
                              cudaStream_t st, int trace_budget);
 
+// ---- path-replay adjoint (adjoint.cu) -----------------------------------------
+constexpr int kAdjSharedMax = 4096;  // material-table gradients kept in shared memory (FP64, 32 KB)
+int adjoint_shared_params(int pmat);
+// adds d(sum of adj-weighted deposits of the pass)/d(params) into grad [M*6*B + E*B*B]
+cudaError_t launch_adjoint(const DevScene &s, const DevConfig &c, uint32_t pass, int band, const double *adj,
+                           double *grad, int *counter, uint32_t *err, int grid, cudaStream_t st);
+// repack material [M][6][B] and/or EEM [E][B][B] tables given as device arrays
+cudaError_t launch_update_materials(float4 *mat, const float *mat_f32, int M, int B, float *eem, float *qy,
+                                    float *cdf, const float *eem_src, int E, cudaStream_t st);
+
 // Allocation-free tile pass (render_wave.cu): scratch from a static device array.
 int noalloc_max_paths();
 size_t noalloc_scratch_bytes();

@@ -330,6 +330,46 @@ class Renderer:
         self._check(self.lib.ts_trace_batch(self._ctx, p(rays), n, m, p(tri), p(t), p(u), p(v), _stream()))
         return tri, t, u, v
 
+    # ---------------------------------------------------------------- differentiation
+    def param_count(self):
+        """(material-table entries M*6*B, EEM entries E*B*B) of the parameter vector."""
+        a, b = ctypes.c_int64(), ctypes.c_int64()
+        self._check(self.lib.ts_param_count(self._ctx, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def update_materials(self, mat_f32=None, eem=None):
+        """Replace the material table [M,6,B] and/or EEM table [E,B,B] (float32 CUDA tensors)."""
+        import torch
+        p = lambda x: None if x is None else ctypes.c_void_p(x.data_ptr())
+        keep = []
+        for x in (mat_f32, eem):
+            if x is not None:
+                if x.device != self.device or x.dtype != torch.float32 or not x.is_contiguous():
+                    raise ValueError("update_materials expects contiguous float32 tensors on the renderer's device")
+                keep.append(x)
+        M, E = self.compiled.mat_f32.shape[0], self.compiled.eem.shape[0]
+        B = self.config.bands
+        if mat_f32 is not None and tuple(mat_f32.shape) != (M, 6, B):
+            raise ValueError(f"mat_f32 must be [{M}, 6, {B}]")
+        if eem is not None and tuple(eem.shape) != (E, B, B):
+            raise ValueError(f"eem must be [{E}, {B}, {B}]")
+        self._check(self.lib.ts_update_materials(self._ctx, p(mat_f32), p(eem), _stream()))
+
+    def adjoint_pass(self, current_sample_in_block, pass_idx, adj, grad):
+        """Path-replay adjoint of cast_rays(current_sample_in_block, pass_idx=pass_idx).
+
+        adj: [B,H,W] float64 CUDA tensor (dLoss / d film cell); grad: [P] float64
+        CUDA tensor, P = sum(param_count()), into which the gradient is ADDED."""
+        import torch
+        c = self.config
+        if adj.dtype != torch.float64 or tuple(adj.shape) != (c.bands, c.height, c.width) or not adj.is_contiguous():
+            raise ValueError("adj must be a contiguous float64 [B, H, W] tensor")
+        if grad.dtype != torch.float64 or grad.numel() != sum(self.param_count()) or not grad.is_contiguous():
+            raise ValueError("grad must be a contiguous float64 tensor of param_count() entries")
+        self._check(self.lib.ts_adjoint_pass(self._ctx, int(pass_idx) & 0xFFFFFFFF, int(current_sample_in_block),
+                                             ctypes.c_void_p(adj.data_ptr()), ctypes.c_void_p(grad.data_ptr()),
+                                             _stream()))
+
     def check_device(self):
         """Raise if a kernel reported an error bit since the last check (synchronises)."""
         bits = ctypes.c_uint32()
