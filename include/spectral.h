@@ -128,6 +128,13 @@ ts_status ts_set_camera(ts_ctx *ctx, const float origin[3], const float lookat[3
  * wavelength index (current_sample_in_block).  Deposits into TS_FILM_BLOCK. */
 ts_status ts_render_pass(ts_ctx *ctx, uint32_t pass_idx, int32_t band, void *stream);
 
+/* num_passes consecutive passes in one launch (a wavelength bundle): pass
+ * first_pass + i renders band (first_band + i) mod B, 1 <= num_passes <= B so
+ * that every pass owns its own film plane; the same paths and deposits as
+ * num_passes ts_render_pass calls.  Small frames fill the GPU this way.  The
+ * wavefront kernel falls back to one launch per pass. */
+ts_status ts_render_passes(ts_ctx *ctx, uint32_t first_pass, int32_t num_passes, int32_t first_band, void *stream);
+
 /* The same pass rendered by the plain megakernel with work counters (used to
  * derive algorithmic bytes per path).  work[0..6] = paths, path vertices,
  * traversals, BVH node visits, triangle tests, hits resolved, film deposits;
@@ -200,6 +207,38 @@ ts_status ts_update_materials(ts_ctx *ctx, const float *mat_f32_dev, const float
  * pass.  scatter_bounces must be <= 16. */
 ts_status ts_adjoint_pass(ts_ctx *ctx, uint32_t pass_idx, int32_t band, const double *adj_dev, double *grad_dev,
                           void *stream);
+/* The adjoint of num_passes consecutive passes (pass first_pass + i at band
+ * (first_band + i) mod B) in one launch; any num_passes >= 1. */
+ts_status ts_adjoint_passes(ts_ctx *ctx, uint32_t first_pass, int32_t num_passes, int32_t first_band,
+                            const double *adj_dev, double *grad_dev, void *stream);
+
+/* ---- batched rendering (new; the reference renders one scene at a time).
+ * Many scenes -- each a context with its own scene, camera, resolution, depth
+ * and film -- rendered by one persistent kernel per step.  A step renders one
+ * whole spectral block of every active scene (band b at pass first_pass +
+ * B*k + b in its k-th step) and then does its average_and_reset_block; the
+ * paths are exactly those of ts_render_pass on each context.  The batch
+ * snapshots the contexts' scenes, cameras and films at creation: contexts must
+ * outlive the batch and keep their scene uploaded.  All scenes must live on
+ * one device and share the BVH width and traversal variant. */
+typedef struct ts_batch ts_batch;
+typedef struct {
+  int32_t block_size;     /* render-kernel threads per block, 32..128 (0 = 128) */
+  int32_t blocks_per_sm;  /* persistent grid = SMs * blocks_per_sm (0 = 5) */
+  int32_t use_graph;      /* 1: capture the step's four kernels as one CUDA graph at the first step, replay after */
+} ts_batch_config;
+
+ts_status ts_batch_create(const ts_batch_config *cfg, ts_ctx *const *ctxs, int32_t num_scenes, ts_batch **out);
+ts_status ts_batch_destroy(ts_batch *batch);
+const char *ts_batch_last_error(const ts_batch *batch);
+/* clear every scene's film and restart its passes at first_pass (synchronises) */
+ts_status ts_batch_reset(ts_batch *batch, uint32_t first_pass, void *stream);
+/* scenes rendered by the next steps: active[num_scenes], nonzero = render (synchronises) */
+ts_status ts_batch_set_active(ts_batch *batch, const int32_t *active, void *stream);
+/* one step: a block of passes for every active scene, then its block average */
+ts_status ts_batch_step(ts_batch *batch, void *stream);
+/* error bits raised by the batch's kernels since the last check (synchronises the device) */
+ts_status ts_batch_check(ts_batch *batch, uint32_t *bits);
 
 /* ---- device status: error bits raised by kernels since the last call (synchronises) */
 ts_status ts_check_device(ts_ctx *ctx, uint32_t *bits);

@@ -73,6 +73,7 @@ SIGNATURES = [
                                          I32P, I32P, I32P, I32P]),
     ("ts_set_camera", ctypes.c_int, [_VP, F32P, F32P, F32P]),
     ("ts_render_pass", ctypes.c_int, [_VP, ctypes.c_uint32, ctypes.c_int32, _VP]),
+    ("ts_render_passes", ctypes.c_int, [_VP, ctypes.c_uint32, ctypes.c_int32, ctypes.c_int32, _VP]),
     ("ts_render_pass_counted", ctypes.c_int, [_VP, ctypes.c_uint32, ctypes.c_int32, _VP,
                                               ctypes.POINTER(ctypes.c_uint64)]),
     ("ts_render_tile_noalloc", ctypes.c_int, [_VP, ctypes.c_uint32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
@@ -90,7 +91,15 @@ SIGNATURES = [
     ("ts_param_count", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]),
     ("ts_update_materials", ctypes.c_int, [_VP, _VP, _VP, _VP]),
     ("ts_adjoint_pass", ctypes.c_int, [_VP, ctypes.c_uint32, ctypes.c_int32, _VP, _VP, _VP]),
+    ("ts_adjoint_passes", ctypes.c_int, [_VP, ctypes.c_uint32, ctypes.c_int32, ctypes.c_int32, _VP, _VP, _VP]),
     ("ts_check_device", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_uint32)]),
+    ("ts_batch_create", ctypes.c_int, [_VP, ctypes.POINTER(_VP), ctypes.c_int32, ctypes.POINTER(_VP)]),
+    ("ts_batch_destroy", ctypes.c_int, [_VP]),
+    ("ts_batch_last_error", ctypes.c_char_p, [_VP]),
+    ("ts_batch_reset", ctypes.c_int, [_VP, ctypes.c_uint32, _VP]),
+    ("ts_batch_set_active", ctypes.c_int, [_VP, I32P, _VP]),
+    ("ts_batch_step", ctypes.c_int, [_VP, _VP]),
+    ("ts_batch_check", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_uint32)]),
 ]
 
 _lib = None

@@ -29,8 +29,7 @@ class _RenderFilm(torch.autograd.Function):
         r.clear_pixel_space()
         B = r.config.bands
         for blk in range(num_blocks):
-            for k in range(B):
-                r.cast_rays(k, pass_idx=first_pass + blk * B + k)
+            r.cast_rays_bundle(0, B, pass_idx=first_pass + blk * B)  # one launch per block
             r.average_and_reset_block(blk + 1)
         film = r.mean_film.clone()
         ctx.renderer = r
@@ -48,13 +47,10 @@ class _RenderFilm(torch.autograd.Function):
         mat, em = ctx.saved_tensors
         # the adjoint replays the forward pass's paths: same tables, same streams
         r.update_materials(mat, em if ctx.has_eem else None)
-        B = r.config.bands
         adj = (grad_film.to(r.device, torch.float64) / ctx.num_blocks).contiguous()
         pm, pe = r.param_count()
         grad = torch.zeros(pm + pe, dtype=torch.float64, device=r.device)
-        for blk in range(ctx.num_blocks):
-            for k in range(B):
-                r.adjoint_pass(k, ctx.first_pass + blk * B + k, adj, grad)
+        r.adjoint_passes(0, ctx.num_blocks * r.config.bands, ctx.first_pass, adj, grad)  # one launch
         gm = grad[:pm].view(mat.shape).to(ctx.mat_dtype)
         ge = grad[pm:].view(r.compiled.eem.shape).to(ctx.eem_dtype) if ctx.has_eem else None
         return gm, ge, None, None, None

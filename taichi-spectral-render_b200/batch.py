@@ -1,0 +1,135 @@
+"""Batched rendering of many scenes in one persistent launch per step.
+
+    batch = Batch([Renderer(scene_i, cfg_i, ...) for i in ...], use_graph=True)
+    batch.reset(first_pass=0)
+    batch.step()             # one spectral block of every active scene, block-averaged
+    batch.set_active(flags)  # drop converged scenes from later steps
+
+Each renderer keeps its own scene, camera, resolution, depth and film; the
+batch renders exactly the paths ``cast_rays`` would render on each of them
+(pass first_pass + B*k + b at band b in step k), so its films equal the
+single-scene renders bit for bit.  ``render_to_rmse`` runs steps until every
+scene's estimated relative XYZ RMSE reaches a target.
+"""
+import ctypes
+import time
+
+import numpy as np
+
+from . import _lib
+from .renderer import _stream
+
+
+class TsBatchConfig(ctypes.Structure):
+    _fields_ = [("block_size", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32), ("use_graph", ctypes.c_int32)]
+
+
+def _check(lib, status, handle):
+    if status != _lib.TS_OK:
+        msg = lib.ts_batch_last_error(handle)
+        raise _lib.SpectralError(status, msg.decode() if msg else "")
+
+
+class Batch:
+    """Scenes (Renderer objects on one device, one BVH width) rendered together."""
+
+    def __init__(self, renderers, block_size=0, blocks_per_sm=0, use_graph=True):
+        self.renderers = list(renderers)
+        self.lib = _lib.load()
+        n = len(self.renderers)
+        arr = (ctypes.c_void_p * n)(*[r._ctx.value for r in self.renderers])
+        cfg = TsBatchConfig(int(block_size), int(blocks_per_sm), 1 if use_graph else 0)
+        self._h = ctypes.c_void_p()
+        _check(self.lib, self.lib.ts_batch_create(ctypes.byref(cfg), arr, n, ctypes.byref(self._h)), None)
+        self.active = np.ones(n, bool)
+        self.blocks = np.zeros(n, np.int64)
+        self.first_pass = 0
+
+    def close(self):
+        if self._h:
+            self.lib.ts_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def reset(self, first_pass=0):
+        """Clear every film; the next step renders passes first_pass .. first_pass + B - 1."""
+        _check(self.lib, self.lib.ts_batch_reset(self._h, int(first_pass) & 0xFFFFFFFF, _stream()), self._h)
+        self.blocks[:] = 0
+        self.first_pass = int(first_pass)
+        for r in self.renderers:
+            r.total_samples = 0
+            r.num_blocks_completed = 0
+
+    def set_active(self, flags):
+        flags = np.asarray(flags, bool)
+        arr = (ctypes.c_int32 * len(flags))(*[int(x) for x in flags])
+        _check(self.lib, self.lib.ts_batch_set_active(self._h, arr, _stream()), self._h)
+        self.active = flags.copy()
+
+    def step(self):
+        """One spectral block of every active scene, followed by its block average."""
+        _check(self.lib, self.lib.ts_batch_step(self._h, _stream()), self._h)
+        self.blocks[self.active] += 1
+        for r, a, nb in zip(self.renderers, self.active, self.blocks):
+            if a:
+                r.total_samples = int(nb) * r.config.bands
+                r.num_blocks_completed = int(nb)
+
+    def check(self):
+        bits = ctypes.c_uint32()
+        _check(self.lib, self.lib.ts_batch_check(self._h, ctypes.byref(bits)), self._h)
+        return bits.value
+
+    def render_to_rmse(self, target=0.01, max_blocks=100000, check_every=1, min_blocks=2, estimator=None):
+        """Steps until every scene's relative XYZ RMSE estimate is <= target.
+
+        Returns per-scene blocks rendered and the wall time (device-synchronised)."""
+        import torch
+        estimator = estimator or relative_rmse_estimate
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        steps = 0
+        while self.active.any():
+            self.step()
+            steps += 1
+            if steps % check_every == 0 or self.blocks.max() >= max_blocks:
+                flags = self.active.copy()
+                for i, r in enumerate(self.renderers):
+                    if flags[i] and self.blocks[i] >= min_blocks:
+                        if self.blocks[i] >= max_blocks or estimator(r, int(self.blocks[i])) <= target:
+                            flags[i] = False
+                if (flags != self.active).any():
+                    self.set_active(flags)
+        torch.cuda.synchronize()
+        return self.blocks.copy(), time.perf_counter() - t0
+
+
+def xyz_mean_and_variance(renderer, nblocks):
+    """Per-pixel XYZ of the block mean and its variance (bands taken as independent), float64 tensors."""
+    import torch
+    n = nblocks
+    mean, m2 = renderer.mean_film, renderer.m2_film
+    cmf = torch.as_tensor(renderer.compiled.cmf, dtype=torch.float64, device=mean.device) * renderer.cmf_scale
+    var = (m2 / n - mean * mean).clamp_min(0.0) * (n / max(n - 1, 1)) / n
+    xyz = torch.einsum("bhw,bc->hwc", mean, cmf)
+    xvar = torch.einsum("bhw,bc->hwc", var, cmf * cmf)
+    return xyz, xvar
+
+
+def relative_rmse_estimate(renderer, nblocks):
+    """sqrt(sum Var(XYZ)) / ||XYZ|| of the block mean: its expected relative RMSE against the converged image."""
+    import torch
+    xyz, xvar = xyz_mean_and_variance(renderer, nblocks)
+    den = float(torch.sum(xyz * xyz))
+    return float(torch.sqrt(torch.sum(xvar))) / max(np.sqrt(den), 1e-300)

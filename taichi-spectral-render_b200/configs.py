@@ -306,3 +306,35 @@ def volume_scene(seed=2, medium_slices=100, medium_stacks=101, width=512, height
               "params": {"sigma_a": sigma_a, "sigma_s": sigma_s, "g": g, "roughness": rough,
                          "albedo_left": rhos[4], "albedo_right": rhos[5]}}
     return {"meshes": meshes, "materials": mats, "camera": camera}, cfg, extras
+
+
+def batch_scene(seed):
+    """One scene of the batched workload, drawn from the box / terrain / volume generators.
+
+    Triangle count log-uniform in 1k-500k, resolution from {128^2, 256^2, 512^2},
+    maximum depth uniform in 4..16; box and terrain scenes are surface-only,
+    volume scenes carry the HG medium (half of them fluorescent)."""
+    rng = np.random.default_rng(seed)
+    tris = float(np.exp(rng.uniform(np.log(1e3), np.log(5e5))))
+    res = int(rng.choice([128, 256, 512]))
+    depth = int(rng.integers(4, 17))
+    kind = str(rng.choice(["box", "terrain", "volume"]))
+    if kind == "box":
+        n = max(8, int(np.sqrt(tris / 2)))
+        out = box_scene(seed=seed, sphere_slices=n, sphere_stacks=n + 1, width=res, height=res, depth=depth)
+    elif kind == "volume":
+        n = max(8, int(np.sqrt(tris / 2)))
+        out = volume_scene(seed=seed, medium_slices=n, medium_stacks=n + 1, width=res, height=res, depth=depth,
+                           fluorescent_medium=bool(rng.integers(2)))
+    else:
+        grid = max(8, int(np.sqrt(0.8 * tris / 2)))
+        n = max(8, int(np.sqrt(0.2 * tris / 2)))
+        out = terrain_scene(seed=seed, grid=grid, sphere_slices=n, sphere_stacks=n + 1, width=res, height=res,
+                            depth=depth)
+    out[2]["kind"] = kind
+    return out
+
+
+def batch_workload(first_seed=100, count=64):
+    """The batched workload: scenes of seeds first_seed .. first_seed + count - 1."""
+    return [batch_scene(s) for s in range(first_seed, first_seed + count)]

@@ -202,7 +202,7 @@ __device__ void grad_surface(const DevScene &s, const DevConfig &c, int pmat, co
 namespace {
 
 template <int W>
-__global__ void __launch_bounds__(128, 4) k_adjoint(DevScene s, DevConfig c, uint32_t pass, int band,
+__global__ void __launch_bounds__(128, 4) k_adjoint(DevScene s, DevConfig c, uint32_t pass0, int npass, int band0,
                                                  const double *__restrict__ adj, double *__restrict__ grad,
                                                  int pm_shared, int pmat, int *__restrict__ counter,
                                                  uint32_t *__restrict__ err) {
@@ -212,9 +212,12 @@ __global__ void __launch_bounds__(128, 4) k_adjoint(DevScene s, DevConfig c, uin
   const Grad g{sh_grad, grad, pm_shared};
   const int lane = threadIdx.x & 31;
   const int npix = c.W * c.H;
+  const int total = npix * npass;
   const int B = c.B;
   uint32_t errbits = 0;
   int pix = -1;
+  uint32_t pass = 0;
+  int band = 0;
   bool exhausted = false;
   int phase = 0;
   PathState p;
@@ -234,12 +237,15 @@ __global__ void __launch_bounds__(128, 4) k_adjoint(DevScene s, DevConfig c, uin
       base = __shfl_sync(0xffffffffu, base, leader);
       if (need) {
         const int idx = base + __popc(m & ((1u << lane) - 1u));
-        if (idx < npix) {
-          pix = idx;
+        if (idx < total) {
+          const int po = idx / npix;
+          pix = idx - po * npix;
+          pass = pass0 + (uint32_t)po;
+          band = (band0 + po) % B;
           phase = 0;
           atot = 0.f;
-          rng.init(c.seed, pass, (uint32_t)idx, c.scene_id);
-          camera_ray(s, c, idx % c.W, idx / c.W, rng, p, band);
+          rng.init(c.seed, pass, (uint32_t)pix, c.scene_id);
+          camera_ray(s, c, pix % c.W, pix / c.W, rng, p, band);
           sp.reset();
           k = 0;
         } else {
@@ -392,7 +398,7 @@ __global__ void __launch_bounds__(128, 4) k_adjoint(DevScene s, DevConfig c, uin
 int adjoint_shared_params(int pmat) { return pmat <= kAdjSharedMax ? pmat : 0; }
 
 cudaError_t launch_adjoint(const DevScene &s, const DevConfig &c, uint32_t pass, int band, const double *adj,
-                           double *grad, int *counter, uint32_t *err, int grid, cudaStream_t st) {
+                           double *grad, int *counter, uint32_t *err, int grid, cudaStream_t st, int npass) {
   cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), st);
   if (e != cudaSuccess) return e;
   const int pmat = s.num_materials * 6 * c.B;
@@ -400,13 +406,13 @@ cudaError_t launch_adjoint(const DevScene &s, const DevConfig &c, uint32_t pass,
   const size_t smem = (size_t)psh * sizeof(double);
   const int block = 128;
   if (s.node_width == 8)
-    k_adjoint<8><<<grid, block, smem, st>>>(s, c, pass, band, adj, grad, psh, pmat, counter, err);
+    k_adjoint<8><<<grid, block, smem, st>>>(s, c, pass, npass, band, adj, grad, psh, pmat, counter, err);
   else if (s.node_width == 4)
-    k_adjoint<4><<<grid, block, smem, st>>>(s, c, pass, band, adj, grad, psh, pmat, counter, err);
+    k_adjoint<4><<<grid, block, smem, st>>>(s, c, pass, npass, band, adj, grad, psh, pmat, counter, err);
   else if (c.speculative)
-    k_adjoint<3><<<grid, block, smem, st>>>(s, c, pass, band, adj, grad, psh, pmat, counter, err);
+    k_adjoint<3><<<grid, block, smem, st>>>(s, c, pass, npass, band, adj, grad, psh, pmat, counter, err);
   else
-    k_adjoint<2><<<grid, block, smem, st>>>(s, c, pass, band, adj, grad, psh, pmat, counter, err);
+    k_adjoint<2><<<grid, block, smem, st>>>(s, c, pass, npass, band, adj, grad, psh, pmat, counter, err);
   return cudaGetLastError();
 }
 

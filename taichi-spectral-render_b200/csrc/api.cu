@@ -11,6 +11,7 @@
 
 #include "bvh.h"
 #include "adjoint.cuh"
+#include "batch.cuh"
 #include "kernels.cuh"
 #include "spectral.h"
 
@@ -477,6 +478,32 @@ ts_status ts_render_pass(ts_ctx *c, uint32_t pass_idx, int32_t band, void *strea
   return TS_OK;
 }
 
+ts_status ts_render_passes(ts_ctx *c, uint32_t first_pass, int32_t num_passes, int32_t first_band, void *stream) {
+  if (!c) return fail(nullptr, TS_ERR_INVALID_ARG, "ts_render_passes: null context");
+  if (!c->has_scene) return fail(c, TS_ERR_NO_SCENE, "ts_render_passes: no scene uploaded");
+  if (first_band < 0 || first_band >= c->cfg.bands)
+    return fail(c, TS_ERR_INVALID_ARG, "ts_render_passes: band out of range");
+  if (num_passes < 1 || num_passes > c->cfg.bands)
+    return fail(c, TS_ERR_INVALID_ARG, "ts_render_passes: num_passes must be 1..bands (one film plane per pass)");
+  if ((int64_t)num_passes * c->cfg.width * c->cfg.height > INT32_MAX)
+    return fail(c, TS_ERR_CAPACITY, "ts_render_passes: more than 2^31 paths in one launch");
+  if (c->cfg.kernel != TS_KERNEL_MEGA) {
+    for (int i = 0; i < num_passes; ++i) {
+      const ts_status st = ts_render_pass(c, first_pass + (uint32_t)i, (first_band + i) % c->cfg.bands, stream);
+      if (st != TS_OK) return st;
+    }
+    return TS_OK;
+  }
+  cudaSetDevice(c->cfg.device);
+  const int bs = c->cfg.block_size;
+  int per_sm = c->cfg.blocks_per_sm;
+  if (per_sm <= 0) per_sm = std::max(1, 2048 / bs);
+  TS_CUDA(c, ts::launch_render_mega(c->ds, c->dc, first_pass, first_band, film_of(c), c->d_counter, c->d_err,
+                                    c->num_sms * per_sm, bs, as_stream(stream), nullptr, num_passes),
+          "ts_render_passes");
+  return TS_OK;
+}
+
 ts_status ts_render_pass_counted(ts_ctx *c, uint32_t pass_idx, int32_t band, void *stream, uint64_t work[8]) {
   if (!c || !work) return fail(c, TS_ERR_INVALID_ARG, "ts_render_pass_counted: bad argument");
   if (!c->has_scene) return fail(c, TS_ERR_NO_SCENE, "ts_render_pass_counted: no scene uploaded");
@@ -636,16 +663,24 @@ ts_status ts_update_materials(ts_ctx *c, const float *mat_f32_dev, const float *
 
 ts_status ts_adjoint_pass(ts_ctx *c, uint32_t pass_idx, int32_t band, const double *adj_dev, double *grad_dev,
                           void *stream) {
+  return ts_adjoint_passes(c, pass_idx, 1, band, adj_dev, grad_dev, stream);
+}
+
+ts_status ts_adjoint_passes(ts_ctx *c, uint32_t first_pass, int32_t num_passes, int32_t band, const double *adj_dev,
+                            double *grad_dev, void *stream) {
   if (!c || !adj_dev || !grad_dev) return fail(c, TS_ERR_INVALID_ARG, "ts_adjoint_pass: null argument");
   if (!c->has_scene) return fail(c, TS_ERR_NO_SCENE, "ts_adjoint_pass: no scene uploaded");
   if (band < 0 || band >= c->cfg.bands) return fail(c, TS_ERR_INVALID_ARG, "ts_adjoint_pass: band out of range");
+  if (num_passes < 1) return fail(c, TS_ERR_INVALID_ARG, "ts_adjoint_passes: num_passes must be positive");
+  if ((int64_t)num_passes * c->cfg.width * c->cfg.height > INT32_MAX)
+    return fail(c, TS_ERR_CAPACITY, "ts_adjoint_passes: more than 2^31 paths in one launch");
   if (c->cfg.scatter_bounces > ts::kAdjMaxSeg)
     return fail(c, TS_ERR_INVALID_ARG, "ts_adjoint_pass: scatter_bounces above " + std::to_string(ts::kAdjMaxSeg) +
                                            " is not supported by the adjoint");
   cudaSetDevice(c->cfg.device);
   const int grid = c->num_sms * 4;
-  TS_CUDA(c, ts::launch_adjoint(c->ds, c->dc, pass_idx, band, adj_dev, grad_dev, c->d_counter, c->d_err, grid,
-                                as_stream(stream)),
+  TS_CUDA(c, ts::launch_adjoint(c->ds, c->dc, first_pass, band, adj_dev, grad_dev, c->d_counter, c->d_err, grid,
+                                as_stream(stream), num_passes),
           "ts_adjoint_pass");
   return TS_OK;
 }
@@ -663,6 +698,182 @@ ts_status ts_check_device(ts_ctx *c, uint32_t *bits) {
     if (*bits & ts::kErrIterationCap) m += " iteration cap reached;";
     return fail(c, TS_ERR_DEVICE_FAULT, m);
   }
+  return TS_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- batches
+struct ts_batch {
+  int device = 0, n = 0, width = 2;
+  ts_batch_config cfg{};
+  int num_sms = 0;
+  std::vector<ts_ctx *> ctxs;
+  std::vector<ts::BatchSlot> host;
+  std::vector<int32_t> active;
+  ts::BatchSlot *d_slots = nullptr;
+  ts::BatchHeader *d_hdr = nullptr;
+  int *d_active = nullptr;
+  uint32_t *d_err = nullptr;
+  cudaStream_t cap = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  std::string err;
+};
+
+namespace {
+ts_status bfail(ts_batch *b, ts_status s, const std::string &msg) {
+  g_last_error = msg;
+  if (b) b->err = msg;
+  return s;
+}
+#define TS_BCUDA(b, expr, what)                                                             \
+  do {                                                                                      \
+    cudaError_t e_ = (expr);                                                                \
+    if (e_ != cudaSuccess)                                                                  \
+      return bfail(b, e_ == cudaErrorMemoryAllocation ? TS_ERR_OUT_OF_MEMORY : TS_ERR_CUDA, \
+                   std::string(what) + ": " + cudaGetErrorString(e_));                      \
+  } while (0)
+
+void batch_free(ts_batch *b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  if (b->cap) cudaStreamDestroy(b->cap);
+  cudaFree(b->d_slots);
+  cudaFree(b->d_hdr);
+  cudaFree(b->d_active);
+  cudaFree(b->d_err);
+}
+
+int batch_width(const ts_ctx *c) { return c->ds.node_width == 2 && c->dc.speculative ? 3 : c->ds.node_width; }
+}  // namespace
+
+extern "C" {
+
+ts_status ts_batch_create(const ts_batch_config *cfg, ts_ctx *const *ctxs, int32_t n, ts_batch **out) {
+  if (!ctxs || !out) return bfail(nullptr, TS_ERR_INVALID_ARG, "ts_batch_create: null argument");
+  *out = nullptr;
+  if (n < 1 || n > ts::kBatchMaxScenes)
+    return bfail(nullptr, TS_ERR_INVALID_ARG,
+                 "ts_batch_create: 1.." + std::to_string(ts::kBatchMaxScenes) + " scenes per batch");
+  for (int i = 0; i < n; ++i) {
+    if (!ctxs[i] || !ctxs[i]->has_scene)
+      return bfail(nullptr, TS_ERR_NO_SCENE, "ts_batch_create: scene " + std::to_string(i) + " has no scene uploaded");
+    if (ctxs[i]->cfg.device != ctxs[0]->cfg.device)
+      return bfail(nullptr, TS_ERR_INVALID_ARG, "ts_batch_create: all scenes must live on one device");
+    if (batch_width(ctxs[i]) != batch_width(ctxs[0]))
+      return bfail(nullptr, TS_ERR_INVALID_ARG,
+                   "ts_batch_create: all scenes of a batch need the same BVH width and traversal variant");
+  }
+  ts_batch *b = new ts_batch();
+  b->device = ctxs[0]->cfg.device;
+  b->n = n;
+  b->width = batch_width(ctxs[0]);
+  if (cfg) b->cfg = *cfg;
+  if (b->cfg.block_size <= 0) b->cfg.block_size = 128;
+  b->cfg.block_size = std::min(128, std::max(32, b->cfg.block_size / 32 * 32));
+  if (b->cfg.blocks_per_sm <= 0) b->cfg.blocks_per_sm = 5;  // the render kernel's resident blocks per SM
+  cudaSetDevice(b->device);
+  cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, b->device);
+  b->ctxs.assign(ctxs, ctxs + n);
+  b->host.resize(n);
+  b->active.assign(n, 1);
+  for (int i = 0; i < n; ++i) {
+    ts::BatchSlot &sl = b->host[i];
+    std::memset(&sl, 0, sizeof(sl));
+    sl.s = ctxs[i]->ds;
+    sl.c = ctxs[i]->dc;
+    sl.f = film_of(ctxs[i]);
+    sl.active = 1;
+  }
+  cudaError_t e = cudaMalloc((void **)&b->d_slots, sizeof(ts::BatchSlot) * n);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&b->d_hdr, sizeof(ts::BatchHeader));
+  if (e == cudaSuccess) e = cudaMalloc((void **)&b->d_active, sizeof(int) * n);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&b->d_err, sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMemset(b->d_err, 0, sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMemcpy(b->d_slots, b->host.data(), sizeof(ts::BatchSlot) * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(b->d_active, b->active.data(), sizeof(int) * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = ts::batch_set_smem_limit(n);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    const std::string msg = std::string("ts_batch_create: ") + cudaGetErrorString(e);
+    batch_free(b);
+    delete b;
+    return bfail(nullptr, e == cudaErrorMemoryAllocation ? TS_ERR_OUT_OF_MEMORY : TS_ERR_CUDA, msg);
+  }
+  *out = b;
+  return TS_OK;
+}
+
+ts_status ts_batch_destroy(ts_batch *b) {
+  if (!b) return TS_OK;
+  cudaSetDevice(b->device);
+  batch_free(b);
+  delete b;
+  return TS_OK;
+}
+
+const char *ts_batch_last_error(const ts_batch *b) { return b ? b->err.c_str() : g_last_error.c_str(); }
+
+ts_status ts_batch_reset(ts_batch *b, uint32_t first_pass, void *stream) {
+  if (!b) return bfail(nullptr, TS_ERR_INVALID_ARG, "ts_batch_reset: null batch");
+  cudaSetDevice(b->device);
+  const cudaStream_t st = as_stream(stream);
+  for (int i = 0; i < b->n; ++i) {
+    TS_BCUDA(b, ts::launch_clear_film(film_of(b->ctxs[i]), st), "ts_batch_reset");
+    b->host[i].pass0 = first_pass;
+    b->host[i].nblocks = 0;
+    b->host[i].active = b->active[i];
+  }
+  TS_BCUDA(b, cudaMemcpyAsync(b->d_slots, b->host.data(), sizeof(ts::BatchSlot) * b->n, cudaMemcpyHostToDevice, st),
+           "ts_batch_reset");
+  TS_BCUDA(b, cudaStreamSynchronize(st), "ts_batch_reset");
+  return TS_OK;
+}
+
+ts_status ts_batch_set_active(ts_batch *b, const int32_t *active, void *stream) {
+  if (!b || !active) return bfail(b, TS_ERR_INVALID_ARG, "ts_batch_set_active: null argument");
+  cudaSetDevice(b->device);
+  for (int i = 0; i < b->n; ++i) b->active[i] = active[i] ? 1 : 0;
+  TS_BCUDA(b, cudaMemcpyAsync(b->d_active, b->active.data(), sizeof(int) * b->n, cudaMemcpyHostToDevice,
+                              as_stream(stream)),
+           "ts_batch_set_active");
+  TS_BCUDA(b, cudaStreamSynchronize(as_stream(stream)), "ts_batch_set_active");
+  return TS_OK;
+}
+
+ts_status ts_batch_step(ts_batch *b, void *stream) {
+  if (!b) return bfail(nullptr, TS_ERR_INVALID_ARG, "ts_batch_step: null batch");
+  cudaSetDevice(b->device);
+  const int grid = b->num_sms * b->cfg.blocks_per_sm;
+  const int acc_blocks = b->num_sms * 2;
+  if (!b->cfg.use_graph) {
+    TS_BCUDA(b, ts::launch_batch_step(b->d_slots, b->n, b->d_hdr, b->d_active, b->d_err, b->width, grid,
+                                      b->cfg.block_size, acc_blocks, as_stream(stream)),
+             "ts_batch_step");
+    return TS_OK;
+  }
+  if (!b->exec) {
+    TS_BCUDA(b, cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal), "ts_batch_step: capture");
+    const cudaError_t le = ts::launch_batch_step(b->d_slots, b->n, b->d_hdr, b->d_active, b->d_err, b->width, grid,
+                                                 b->cfg.block_size, acc_blocks, b->cap);
+    const cudaError_t ce = cudaStreamEndCapture(b->cap, &b->graph);
+    TS_BCUDA(b, le, "ts_batch_step: capture");
+    TS_BCUDA(b, ce, "ts_batch_step: capture");
+    TS_BCUDA(b, cudaGraphInstantiate(&b->exec, b->graph, 0), "ts_batch_step: graph instantiation");
+  }
+  TS_BCUDA(b, cudaGraphLaunch(b->exec, as_stream(stream)), "ts_batch_step: graph launch");
+  return TS_OK;
+}
+
+ts_status ts_batch_check(ts_batch *b, uint32_t *bits) {
+  if (!b || !bits) return bfail(b, TS_ERR_INVALID_ARG, "ts_batch_check: null argument");
+  cudaSetDevice(b->device);
+  TS_BCUDA(b, cudaDeviceSynchronize(), "ts_batch_check");
+  TS_BCUDA(b, cudaMemcpy(bits, b->d_err, sizeof(uint32_t), cudaMemcpyDeviceToHost), "ts_batch_check");
+  TS_BCUDA(b, cudaMemset(b->d_err, 0, sizeof(uint32_t)), "ts_batch_check");
+  if (*bits)
+    return bfail(b, TS_ERR_DEVICE_FAULT, "ts_batch_check: a kernel reported error bits " + std::to_string(*bits));
   return TS_OK;
 }
 

@@ -16,11 +16,12 @@ struct Film {
   int W, H, B;
 };
 
-// one sample pass (cast_rays): persistent megakernel with per-lane path regeneration
+// npass consecutive sample passes (cast_rays) from pass / band, band wrapping
+// mod B (npass <= B): persistent megakernel with per-lane path regeneration.
 // work != nullptr selects the counting variant (work[8], accumulated)
 cudaError_t launch_render_mega(const DevScene &s, const DevConfig &c, uint32_t pass, int band, Film f,
                                int *counter, uint32_t *err, int grid, int block, cudaStream_t st,
-                               unsigned long long *work = nullptr);
+                               unsigned long long *work = nullptr, int npass = 1);
 
 // closest hit for a ray batch; mode 0 = fast traversal, 1 = reference order
 cudaError_t launch_trace_batch(const DevScene &s, float eps, const float *rays, int n, int mode, int32_t *tri_orig,
@@ -65,7 +66,7 @@ constexpr int kAdjSharedMax = 4096;  // material-table gradients kept in shared 
 int adjoint_shared_params(int pmat);
 // adds d(sum of adj-weighted deposits of the pass)/d(params) into grad [M*6*B + E*B*B]
 cudaError_t launch_adjoint(const DevScene &s, const DevConfig &c, uint32_t pass, int band, const double *adj,
-                           double *grad, int *counter, uint32_t *err, int grid, cudaStream_t st);
+                           double *grad, int *counter, uint32_t *err, int grid, cudaStream_t st, int npass = 1);
 // repack material [M][6][B] and/or EEM [E][B][B] tables given as device arrays
 cudaError_t launch_update_materials(float4 *mat, const float *mat_f32, int M, int B, float *eem, float *qy,
                                     float *cdf, const float *eem_src, int E, cudaStream_t st);

@@ -189,6 +189,15 @@ class Renderer:
                                             _stream()))
         self.total_samples += 1
 
+    def cast_rays_bundle(self, first_band, num_passes, pass_idx=None):
+        """num_passes consecutive passes (bands first_band, first_band + 1, ... mod B) in one
+        launch: the same paths as num_passes cast_rays calls (num_passes <= bands)."""
+        if pass_idx is None:
+            pass_idx = self.total_samples
+        self._check(self.lib.ts_render_passes(self._ctx, int(pass_idx) & 0xFFFFFFFF, int(num_passes),
+                                              int(first_band), _stream()))
+        self.total_samples += int(num_passes)
+
     def cast_rays_counted(self, current_sample_in_block, pass_idx=None):
         """cast_rays through the counting megakernel; returns the work counts."""
         if pass_idx is None:
@@ -369,6 +378,18 @@ class Renderer:
         self._check(self.lib.ts_adjoint_pass(self._ctx, int(pass_idx) & 0xFFFFFFFF, int(current_sample_in_block),
                                              ctypes.c_void_p(adj.data_ptr()), ctypes.c_void_p(grad.data_ptr()),
                                              _stream()))
+
+    def adjoint_passes(self, first_band, num_passes, first_pass, adj, grad):
+        """adjoint_pass over num_passes consecutive passes in one launch."""
+        import torch
+        c = self.config
+        if adj.dtype != torch.float64 or tuple(adj.shape) != (c.bands, c.height, c.width) or not adj.is_contiguous():
+            raise ValueError("adj must be a contiguous float64 [B, H, W] tensor")
+        if grad.dtype != torch.float64 or grad.numel() != sum(self.param_count()) or not grad.is_contiguous():
+            raise ValueError("grad must be a contiguous float64 tensor of param_count() entries")
+        self._check(self.lib.ts_adjoint_passes(self._ctx, int(first_pass) & 0xFFFFFFFF, int(num_passes),
+                                               int(first_band), ctypes.c_void_p(adj.data_ptr()),
+                                               ctypes.c_void_p(grad.data_ptr()), _stream()))
 
     def check_device(self):
         """Raise if a kernel reported an error bit since the last check (synchronises)."""
