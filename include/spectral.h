@@ -131,7 +131,8 @@ ts_status ts_render_pass(ts_ctx *ctx, uint32_t pass_idx, int32_t band, void *str
 /* num_passes consecutive passes in one launch (a wavelength bundle): pass
  * first_pass + i renders band (first_band + i) mod B, 1 <= num_passes <= B so
  * that every pass owns its own film plane; the same paths and deposits as
- * num_passes ts_render_pass calls.  Small frames fill the GPU this way.  The
+ * num_passes ts_render_pass calls (film sums equal up to the order of FP64
+ * additions where volume fluorescence moves deposits between bands).  Small frames fill the GPU this way.  The
  * wavefront kernel falls back to one launch per pass. */
 ts_status ts_render_passes(ts_ctx *ctx, uint32_t first_pass, int32_t num_passes, int32_t first_band, void *stream);
 
@@ -217,7 +218,9 @@ ts_status ts_adjoint_passes(ts_ctx *ctx, uint32_t first_pass, int32_t num_passes
  * and film -- rendered by one persistent kernel per step.  A step renders one
  * whole spectral block of every active scene (band b at pass first_pass +
  * B*k + b in its k-th step) and then does its average_and_reset_block; the
- * paths are exactly those of ts_render_pass on each context.  The batch
+ * paths are exactly those of ts_render_pass on each context (film sums equal
+ * up to the order of FP64 additions where fluorescence moves deposits between
+ * bands).  The batch
  * snapshots the contexts' scenes, cameras and films at creation: contexts must
  * outlive the batch and keep their scene uploaded.  All scenes must live on
  * one device and share the BVH width and traversal variant. */

@@ -6,8 +6,11 @@
 // loop iteration per call: the extension trace of scatter_volume, the
 // volume/surface event, next-event estimation with its shadow chain and the
 // surface scatter.  Deposits of the path are summed in FP64 and written to the
-// film when the path ends or changes band (one owner lane per film cell and
-// pass, so plain read-modify-writes suffice).
+// film when the path ends or changes band.  With one pass per launch a film
+// cell has one owner lane and a plain read-modify-write suffices; a launch of
+// several passes shares cells -- volume fluorescence moves a path's deposits
+// to another band, i.e. into the plane of another pass of the launch -- so it
+// flushes with FP64 atomics (shared = true).
 #pragma once
 #include "estimator.cuh"
 #include "kernels.cuh"
@@ -29,10 +32,11 @@ struct MegaCounts {
   uint32_t paths = 0, vert = 0, trace = 0, hit = 0, dep = 0;
 };
 
-__device__ __forceinline__ void mega_flush(const Film &f, int pixel, int band, double dep) {
+__device__ __forceinline__ void mega_flush(const Film &f, int pixel, int band, double dep, bool shared) {
   if (dep != 0.0 || dep != dep) {
     double *cell = f.block + (size_t)band * f.W * f.H + pixel;
-    *cell += dep;  // one owner lane per pixel, band and launch
+    if (shared) atomicAdd(cell, dep);
+    else *cell += dep;  // one owner lane per pixel, band and launch
   }
 }
 
@@ -49,7 +53,7 @@ __device__ __forceinline__ void mega_start(const DevScene &s, const DevConfig &c
 // Returns true when the path has ended (its deposit flushed).
 template <int W, bool kCount>
 __device__ __forceinline__ bool mega_vertex(const DevScene &s, const DevConfig &c, const Film &f, MegaLane &L,
-                                            uint32_t &errbits, MegaCounts &cnt) {
+                                            uint32_t &errbits, MegaCounts &cnt, bool shared) {
   PathState &p = L.p;
   const int band = L.band;
   bool done = false;
@@ -108,7 +112,7 @@ __device__ __forceinline__ bool mega_vertex(const DevScene &s, const DevConfig &
     } else if (ev.action == 3) {
       p.dir = ev.dir;
       if (kCount) cnt.dep += L.dep != 0.0;
-      mega_flush(f, L.pix, p.active_px, L.dep);
+      mega_flush(f, L.pix, p.active_px, L.dep, shared);
       L.dep = 0.0;
       p.active = ev.new_wl;
       p.active_px = ev.new_wl;
@@ -122,7 +126,7 @@ __device__ __forceinline__ bool mega_vertex(const DevScene &s, const DevConfig &
   }
   if (done) {
     if (kCount) cnt.dep += L.dep != 0.0;
-    mega_flush(f, L.pix, p.active_px, L.dep);
+    mega_flush(f, L.pix, p.active_px, L.dep, shared);
     L.pix = -1;
   }
   return done;

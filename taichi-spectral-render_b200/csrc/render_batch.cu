@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(128, 5) k_render_batch(const BatchSlot *__rest
     if (__ballot_sync(0xffffffffu, L.pix >= 0) == 0) break;
     if (L.pix < 0) continue;
     const BatchSlot &sl = sh[slot];
-    mega_vertex<W, false>(sl.s, sl.c, sl.f, L, errbits, cnt);
+    mega_vertex<W, false>(sl.s, sl.c, sl.f, L, errbits, cnt, true);
   }
   if (errbits) atomicOr(err, errbits);
 }

@@ -7,7 +7,8 @@
 // idling behind its longest path.  A launch covers npass consecutive passes
 // (a wavelength bundle): work item idx is pixel idx % npix of pass
 // pass0 + idx / npix at band (band0 + idx / npix) mod B.  Bands of one launch
-// are distinct, so every film cell still has one owner lane.
+// are distinct; fluorescence can still move deposits into another pass's band,
+// so multi-pass launches flush with atomics.
 #include "mega_path.cuh"
 
 namespace ts {
@@ -52,7 +53,7 @@ __global__ void __launch_bounds__(128, 5) k_render_mega(DevScene s, DevConfig c,
     }
     if (__ballot_sync(0xffffffffu, L.pix >= 0) == 0) break;
     if (L.pix < 0) continue;
-    mega_vertex<W, kCount>(s, c, f, L, errbits, cnt);
+    mega_vertex<W, kCount>(s, c, f, L, errbits, cnt, npass > 1);
   }
   if (errbits) atomicOr(err, errbits);
   if (kCount) {

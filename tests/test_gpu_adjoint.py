@@ -135,7 +135,8 @@ def test_autograd_render_film():
             r.cast_rays(k % B, pass_idx=50 + k)
             if (k + 1) % B == 0:
                 r.average_and_reset_block((k + 1) // B)
-        assert torch.equal(film, r.mean_film)
+        # equal up to the order of the FP64 additions of fluorescence-shifted deposits
+        assert torch.allclose(film, r.mean_film, rtol=1e-12, atol=0)
         xyz = autodiff.film_to_xyz(film, comp.cmf, r.cmf_scale)
         target = torch.zeros_like(xyz)
         loss = ((xyz - target) ** 2).sum()

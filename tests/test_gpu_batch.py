@@ -23,6 +23,12 @@ def renderer(args):
     return sb.Renderer(s, c, eems=ex["eems"], cmf=ex["cmf"], bvh=bvh)
 
 
+def same_film(a, b):
+    """Equal up to the order of FP64 additions (volume fluorescence lets two passes of
+    one launch deposit into the same cell, which they add atomically in either order)."""
+    return torch.allclose(a, b, rtol=1e-12, atol=0)
+
+
 def single_scene_mean(args, blocks, first_pass=0):
     with renderer(args) as r:
         B = r.config.bands
@@ -44,14 +50,14 @@ SCENES = [
 
 
 def test_bundle_equals_single_passes():
-    args = make(*SCENES[1])
+    args = make(SCENES[1][0], **SCENES[1][1])
     ref = single_scene_mean(args, 2, first_pass=40)
     with renderer(args) as r:
         B = r.config.bands
         for blk in range(2):
             r.cast_rays_bundle(0, B, pass_idx=40 + blk * B)
             r.average_and_reset_block(blk + 1)
-        assert torch.equal(r.mean_film, ref[0]) and torch.equal(r.m2_film, ref[1])
+        assert same_film(r.mean_film, ref[0]) and same_film(r.m2_film, ref[1])
         # a partial bundle from the middle of the band range, wrapping past the last band
         r.clear_pixel_space()
         r.cast_rays_bundle(20, 10, pass_idx=7)
@@ -59,13 +65,13 @@ def test_bundle_equals_single_passes():
         r.clear_pixel_space()
         for i in range(10):
             r.cast_rays((20 + i) % B, pass_idx=7 + i)
-        assert torch.equal(r.block_film, a)
+        assert same_film(r.block_film, a)
         with pytest.raises(sb.SpectralError):
             r.cast_rays_bundle(0, B + 1, pass_idx=0)
 
 
 def test_adjoint_bundle_equals_single_passes():
-    args = make(*SCENES[1])
+    args = make(SCENES[1][0], **SCENES[1][1])
     with renderer(args) as r:
         B = r.config.bands
         pm, pe = r.param_count()
@@ -89,9 +95,11 @@ def test_batch_equals_single_scene_renders(use_graph):
         for _ in range(3):
             b.step()
         assert b.check() == 0
-        for r, (mean, m2) in zip(rs, refs):
-            assert torch.equal(r.mean_film, mean)
-            assert torch.equal(r.m2_film, m2)
+        for i, (r, (mean, m2)) in enumerate(zip(rs, refs)):
+            if i == 1:  # fluorescent medium
+                assert same_film(r.mean_film, mean) and same_film(r.m2_film, m2)
+            else:  # one deposit per cell and launch: bit for bit
+                assert torch.equal(r.mean_film, mean) and torch.equal(r.m2_film, m2)
         # an inactive scene keeps its film while the others advance
         keep = rs[1].mean_film.clone()
         b.set_active([True, False, True])
@@ -119,8 +127,8 @@ def test_render_to_rmse_stops_each_scene():
 
 
 def test_batch_rejects_mixed_bvh_widths():
-    a = make(*SCENES[0])
-    s, c, ex, _ = make(*SCENES[2])
+    a = make(SCENES[0][0], **SCENES[0][1])
+    s, c, ex, _ = make(SCENES[2][0], **SCENES[2][1])
     r1 = renderer(a)
     r2 = sb.Renderer(s, c, eems=ex["eems"], cmf=ex["cmf"], bvh_params={"width": 4})
     with pytest.raises(sb.SpectralError):
