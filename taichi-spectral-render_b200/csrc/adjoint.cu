@@ -3,10 +3,11 @@
 // capability; the reference renderer, main.py of Xyzonox/taichi-spectral-render,
 // has none).
 //
-// Each lane owns one path of cast_rays (main.py:1502-1590) and runs it twice
-// from its Philox stream (path replay, no tape):
+// Each path of cast_rays (main.py:1502-1590) runs twice from its Philox
+// stream (path replay, no tape), in two launches of the same persistent kernel:
 //   replay 0: the path as the forward pass rendered it, summing its deposits
-//             weighted by the adjoint film, A = sum_v w(pixel, band_v) D_v;
+//             weighted by the adjoint film, A = sum_v w(pixel, band_v) D_v,
+//             stored per path (4 bytes);
 //   replay 1: the same path again.  A_rem starts at A and drops by w D_v at
 //             each deposit.  Every multiplicative factor f of the throughput
 //             and every sampling decision with probability p adds
@@ -14,9 +15,12 @@
 //             is then exactly the weighted radiance the factor scales -- and
 //             every deposit adds w * dD_v for its own factors (emission,
 //             BSDF / phase function, MIS weight, shadow transmittance).
-// Path arithmetic is FP32 like the forward kernels (the same event functions,
-// so the replays take the forward pass's branches); gradient sums are FP64,
-// per block in shared memory, then across blocks with global atomics.
+// The phase is a template parameter: replay 0 carries no gradient code and
+// every lane of a replay-1 warp executes the gradient code (one launch mixing
+// the phases per lane ran them divergently).  Path arithmetic is FP32 like the
+// forward kernels (the same event functions, so the replays take the forward
+// pass's branches); gradient sums are FP64, per block in shared memory, then
+// across blocks with global atomics.
 #include "adjoint.cuh"
 #include "kernels.cuh"
 
@@ -201,11 +205,11 @@ __device__ void grad_surface(const DevScene &s, const DevConfig &c, int pmat, co
 
 namespace {
 
-template <int W>
-__global__ void __launch_bounds__(128, 4) k_adjoint(DevScene s, DevConfig c, uint32_t pass0, int npass, int band0,
+template <int W, int kPhase>
+__global__ void __launch_bounds__(128, kPhase ? 4 : 5) k_adjoint(DevScene s, DevConfig c, uint32_t pass0, int npass, int band0,
                                                  const double *__restrict__ adj, double *__restrict__ grad,
-                                                 int pm_shared, int pmat, int *__restrict__ counter,
-                                                 uint32_t *__restrict__ err) {
+                                                 float *__restrict__ weight, int pm_shared, int pmat,
+                                                 int *__restrict__ counter, uint32_t *__restrict__ err) {
   extern __shared__ double sh_grad[];
   for (int i = threadIdx.x; i < pm_shared; i += blockDim.x) sh_grad[i] = 0.0;
   __syncthreads();
@@ -219,7 +223,8 @@ __global__ void __launch_bounds__(128, 4) k_adjoint(DevScene s, DevConfig c, uin
   uint32_t pass = 0;
   int band = 0;
   bool exhausted = false;
-  int phase = 0;
+  constexpr bool phase = kPhase == 1;
+  int item = 0;
   PathState p;
   Rng rng;
   SpdfGrad sp;
@@ -242,8 +247,9 @@ __global__ void __launch_bounds__(128, 4) k_adjoint(DevScene s, DevConfig c, uin
           pix = idx - po * npix;
           pass = pass0 + (uint32_t)po;
           band = (band0 + po) % B;
-          phase = 0;
+          item = idx;
           atot = 0.f;
+          if (phase) arem = weight[idx];
           rng.init(c.seed, pass, (uint32_t)pix, c.scene_id);
           camera_ray(s, c, pix % c.W, pix / c.W, rng, p, band);
           sp.reset();
@@ -374,17 +380,8 @@ __global__ void __launch_bounds__(128, 4) k_adjoint(DevScene s, DevConfig c, uin
       if (++k >= c.max_depth || p.thr == 0.f) done = true;
     }
     if (done) {
-      if (phase == 0) {
-        // replay the same path with gradients
-        phase = 1;
-        arem = atot;
-        rng.init(c.seed, pass, (uint32_t)pix, c.scene_id);
-        camera_ray(s, c, pix % c.W, pix / c.W, rng, p, band);
-        sp.reset();
-        k = 0;
-      } else {
-        pix = -1;
-      }
+      if (!phase) weight[item] = atot;  // replay 1 starts from this
+      pix = -1;
     }
   }
   if (errbits) atomicOr(err, errbits);
@@ -397,22 +394,31 @@ __global__ void __launch_bounds__(128, 4) k_adjoint(DevScene s, DevConfig c, uin
 
 int adjoint_shared_params(int pmat) { return pmat <= kAdjSharedMax ? pmat : 0; }
 
+namespace {
+template <int W>
+void launch_pair(const DevScene &s, const DevConfig &c, uint32_t pass, int npass, int band, const double *adj,
+                 double *grad, float *weight, int psh, int pmat, int *counter, uint32_t *err, int grid,
+                 cudaStream_t st) {
+  const int block = 128;
+  k_adjoint<W, 0><<<grid, block, 0, st>>>(s, c, pass, npass, band, adj, grad, weight, 0, pmat, counter, err);
+  k_adjoint<W, 1><<<grid, block, (size_t)psh * sizeof(double), st>>>(s, c, pass, npass, band, adj, grad, weight, psh,
+                                                                     pmat, counter + 1, err);
+}
+}  // namespace
+
 cudaError_t launch_adjoint(const DevScene &s, const DevConfig &c, uint32_t pass, int band, const double *adj,
-                           double *grad, int *counter, uint32_t *err, int grid, cudaStream_t st, int npass) {
-  cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), st);
+                           double *grad, float *weight, int *counter, uint32_t *err, int grid, cudaStream_t st,
+                           int npass) {
+  cudaError_t e = cudaMemsetAsync(counter, 0, 2 * sizeof(int), st);
   if (e != cudaSuccess) return e;
   const int pmat = s.num_materials * 6 * c.B;
   const int psh = adjoint_shared_params(pmat);
-  const size_t smem = (size_t)psh * sizeof(double);
-  const int block = 128;
-  if (s.node_width == 8)
-    k_adjoint<8><<<grid, block, smem, st>>>(s, c, pass, npass, band, adj, grad, psh, pmat, counter, err);
+  if (s.node_width == 8) launch_pair<8>(s, c, pass, npass, band, adj, grad, weight, psh, pmat, counter, err, grid, st);
   else if (s.node_width == 4)
-    k_adjoint<4><<<grid, block, smem, st>>>(s, c, pass, npass, band, adj, grad, psh, pmat, counter, err);
+    launch_pair<4>(s, c, pass, npass, band, adj, grad, weight, psh, pmat, counter, err, grid, st);
   else if (c.speculative)
-    k_adjoint<3><<<grid, block, smem, st>>>(s, c, pass, npass, band, adj, grad, psh, pmat, counter, err);
-  else
-    k_adjoint<2><<<grid, block, smem, st>>>(s, c, pass, npass, band, adj, grad, psh, pmat, counter, err);
+    launch_pair<3>(s, c, pass, npass, band, adj, grad, weight, psh, pmat, counter, err, grid, st);
+  else launch_pair<2>(s, c, pass, npass, band, adj, grad, weight, psh, pmat, counter, err, grid, st);
   return cudaGetLastError();
 }
 

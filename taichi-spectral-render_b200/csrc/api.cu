@@ -41,6 +41,8 @@ struct ts_ctx {
   float *d_m9 = nullptr;  // XYZ->RGB matrix for ts_resolve_rgb
   float4 *d_mat = nullptr;  // packed material table (scene allocation), rewritten by ts_update_materials
   float *d_eem = nullptr, *d_qy = nullptr, *d_cdf = nullptr;
+  float *d_adj_weight = nullptr;  // adjoint scratch: per-path weighted totals
+  size_t adj_weight_cap = 0;      // entries
   ts::WaveBuffers wave{};
   std::vector<void *> wave_allocs;
   size_t film_bytes = 0, scene_bytes = 0, wave_bytes = 0;
@@ -195,6 +197,7 @@ ts_status ts_destroy(ts_ctx *c) {
   cudaFree(c->d_err);
   cudaFree(c->d_xyz);
   cudaFree(c->d_m9);
+  cudaFree(c->d_adj_weight);
   delete c;
   return TS_OK;
 }
@@ -679,9 +682,24 @@ ts_status ts_adjoint_passes(ts_ctx *c, uint32_t first_pass, int32_t num_passes, 
                                            " is not supported by the adjoint");
   cudaSetDevice(c->cfg.device);
   const int grid = c->num_sms * 4;
-  TS_CUDA(c, ts::launch_adjoint(c->ds, c->dc, first_pass, band, adj_dev, grad_dev, c->d_counter, c->d_err, grid,
-                                as_stream(stream), num_passes),
-          "ts_adjoint_pass");
+  // the two replays pass each path's weighted total through device scratch;
+  // launches are chunked so that it stays <= 64 MB
+  const int64_t npix = (int64_t)c->cfg.width * c->cfg.height;
+  const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(num_passes, ts::kAdjMaxPathsPerLaunch / npix));
+  const size_t need = (size_t)(chunk * npix);
+  if (need > c->adj_weight_cap) {
+    cudaFree(c->d_adj_weight);
+    c->d_adj_weight = nullptr;
+    c->adj_weight_cap = 0;
+    TS_CUDA(c, cudaMalloc((void **)&c->d_adj_weight, need * sizeof(float)), "ts_adjoint_pass: scratch");
+    c->adj_weight_cap = need;
+  }
+  for (int64_t p0 = 0; p0 < num_passes; p0 += chunk) {
+    const int n = (int)std::min<int64_t>(chunk, num_passes - p0);
+    TS_CUDA(c, ts::launch_adjoint(c->ds, c->dc, first_pass + (uint32_t)p0, (int)((band + p0) % c->cfg.bands), adj_dev,
+                                  grad_dev, c->d_adj_weight, c->d_counter, c->d_err, grid, as_stream(stream), n),
+            "ts_adjoint_pass");
+  }
   return TS_OK;
 }
 

@@ -65,8 +65,11 @@ cudaError_t launch_wave_pass(const DevScene &s, const DevConfig &c, uint32_t pas
 constexpr int kAdjSharedMax = 4096;  // material-table gradients kept in shared memory (FP64, 32 KB)
 int adjoint_shared_params(int pmat);
 // adds d(sum of adj-weighted deposits of the pass)/d(params) into grad [M*6*B + E*B*B]
+// weight: [npass * W * H] float scratch (each path's adjoint-weighted total); counter: 2 ints
+constexpr int kAdjMaxPathsPerLaunch = 1 << 24;  // bounds the weight scratch at 64 MB
 cudaError_t launch_adjoint(const DevScene &s, const DevConfig &c, uint32_t pass, int band, const double *adj,
-                           double *grad, int *counter, uint32_t *err, int grid, cudaStream_t st, int npass = 1);
+                           double *grad, float *weight, int *counter, uint32_t *err, int grid, cudaStream_t st,
+                           int npass = 1);
 // repack material [M][6][B] and/or EEM [E][B][B] tables given as device arrays
 cudaError_t launch_update_materials(float4 *mat, const float *mat_f32, int M, int B, float *eem, float *qy,
                                     float *cdf, const float *eem_src, int E, cudaStream_t st);

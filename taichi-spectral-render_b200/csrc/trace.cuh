@@ -381,9 +381,12 @@ struct StackSize {
 // Fast closest hit in one go (local-memory stack).  errbits gets
 // kErrStackOverflow if the tree is deeper than the stack (the builder bounds
 // the depth below it, so this is a guard only).
+// Not inlined: one copy of the traversal per kernel instead of one per call
+// site keeps the megakernels' instruction footprint small (instruction-fetch
+// stalls dominated them when inlined).
 template <int W, bool kCount = false>
-TS_D Hit trace_closest(const DevScene &s, float3 o, float3 d, float eps, uint32_t &errbits, TraceCount *tc = nullptr,
-                       float bound = 1e9f) {
+__device__ __noinline__ Hit trace_closest(const DevScene &s, float3 o, float3 d, float eps, uint32_t &errbits,
+                                          TraceCount *tc = nullptr, float bound = 1e9f) {
   Traversal t;
   int2 stack[StackSize<W>::value];
   trav_begin(s, t, o, d, bound);
