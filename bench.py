@@ -40,11 +40,15 @@ def parse():
     p.add_argument("--warmup", type=int, default=10)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--kernel", default="mega", choices=["mega", "wavefront"])
-    p.add_argument("--workload", default="terrain", choices=["terrain", "box", "volume"])
+    p.add_argument("--workload", default="terrain", choices=["terrain", "box", "volume", "batch"])
     p.add_argument("--width", type=int, default=2, choices=[2, 4, 8], help="BVH node width")
     p.add_argument("--traversal", default="default", choices=["default", "speculative"])
     p.add_argument("--budget", type=int, default=0, help="wavefront traversal steps between refills")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-extras", action="store_true", help="skip the time-to-RMSE and adjoint-cost legs")
+    p.add_argument("--rmse-seconds", type=float, default=60.0, help="time limit of each time-to-RMSE leg")
+    p.add_argument("--batch-scenes", type=int, default=64, help="scenes of the batched workload (--workload batch)")
+    p.add_argument("--batch-target", type=float, default=0.05, help="RMSE target of the batched workload")
     return p.parse_args()
 
 
@@ -168,6 +172,179 @@ def cpu_oracle_rate(comp, bvh, scene, cfg, seconds, nthreads=0, passes=None):
     dt = time.perf_counter() - t
     threads = nthreads if nthreads > 0 else (os.cpu_count() or 1)
     return n / dt, n, dt, threads, st
+
+
+def oracle_fixture(name):
+    path = os.path.join(ROOT, "tests", "golden", f"oracle_{name}.npz")
+    if not os.path.exists(path):
+        return None
+    import numpy as np
+    return dict(np.load(path))
+
+
+def rmse_leg(name, target, seconds, bundles=True):
+    """Blocks until the image's estimated relative XYZ RMSE (its own per-pixel
+    variance; the GPU estimator is unbiased) reaches ``target``, or ``seconds``
+    run out; then the image is compared with the FP64 oracle fixture on the
+    oracle's pixel subset (independent random streams): the difference must
+    match the combined noise of both images (z near 0 means no bias)."""
+    import numpy as np
+    import torch
+    import spectral_b200 as sb
+    from spectral_b200 import batch as sbatch
+    scene, cfg, ex, desc = workload(name)
+    cfg.kernel = "mega"
+    r = sb.Renderer(scene, cfg, eems=ex["eems"], cmf=ex["cmf"])
+    B = cfg.bands
+    r.cast_rays_bundle(0, B, pass_idx=0)
+    r.clear_pixel_space()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    nb, est = 0, float("inf")
+    next_check = 2
+    while True:
+        if bundles:
+            r.cast_rays_bundle(0, B, pass_idx=nb * B)
+        else:
+            for k in range(B):
+                r.cast_rays(k, pass_idx=nb * B + k)
+        nb += 1
+        r.average_and_reset_block(nb)
+        if nb >= next_check:
+            est = sbatch.relative_rmse_estimate(r, nb)
+            if est <= target:
+                break
+            # next check where 1/sqrt(n) scaling predicts the target (at most doubling n)
+            next_check = nb + max(1, min(nb, int(nb * ((est / target) ** 2 - 1) * 0.9)))
+        if time.perf_counter() - t0 > seconds:
+            break
+    torch.cuda.synchronize()
+    secs = time.perf_counter() - t0
+    est = sbatch.relative_rmse_estimate(r, nb)
+    out = {"workload": name, "target": target, "blocks": nb, "spp": nb * B, "seconds": secs,
+           "estimated_rmse": float(est), "reached": bool(est <= target),
+           "launches": "one per block (wavelength bundle)" if bundles else "one per pass"}
+    if est > target:
+        # time to a target scales with its inverse square (variance ~ 1 / samples)
+        out["seconds_extrapolated"] = secs * (est / target) ** 2
+    fx = oracle_fixture(name)
+    if fx is not None:
+        xyz, xvar = sbatch.xyz_mean_and_variance(r, nb)
+        W = cfg.width
+        pix = fx["pixels"].astype(np.int64)
+        g = xyz.reshape(-1, 3)[torch.as_tensor(pix, device=xyz.device)].cpu().numpy()
+        gv = xvar.reshape(-1, 3)[torch.as_tensor(pix, device=xyz.device)].cpu().numpy()
+        o = fx["xyz"].astype(np.float64)
+        cmf = np.asarray(r.compiled.cmf, np.float64) * r.cmf_scale
+        ov = (fx["sem"].astype(np.float64) ** 2) @ (cmf ** 2)
+        norm = np.sqrt((o ** 2).sum())
+        diff2 = ((g - o) ** 2).sum()
+        expect2 = gv.sum() + ov.sum()
+        # per-pixel sums of squared differences: spread of the difference statistic
+        d2 = ((g - o) ** 2).sum(1)
+        se2 = np.sqrt(max(float(((d2 - d2.mean()) ** 2).sum()), 1e-300))
+        out["vs_oracle"] = {"oracle_spp": int(fx["spp"]), "pixels": int(pix.shape[0]),
+                            "rmse_vs_oracle": float(np.sqrt(diff2) / norm),
+                            "expected_from_noise": float(np.sqrt(expect2) / norm),
+                            "oracle_noise_rmse": float(np.sqrt(ov.sum()) / norm),
+                            "z": float((diff2 - expect2) / se2)}
+    bits = r.check_device()
+    r.close()
+    out["device_error_bits"] = bits
+    return out
+
+
+def adjoint_leg():
+    """Cost of the path-replay adjoint against the forward pass on the
+    inverse-rendering scene (box + HG medium + fluorescent wall, 256^2, depth 32)."""
+    import torch
+    import spectral_b200 as sb
+    from spectral_b200 import configs
+    s, c, ex = configs.volume_scene(width=256, height=256, depth=32)
+    c.kernel = "mega"
+    r = sb.Renderer(s, c, eems=ex["eems"], cmf=ex["cmf"])
+    B = c.bands
+    pm, pe = r.param_count()
+    adj = torch.rand((B, c.height, c.width), dtype=torch.float64, device="cuda")
+    g = torch.zeros(pm + pe, dtype=torch.float64, device="cuda")
+    r.cast_rays_bundle(0, B, pass_idx=0)
+    r.adjoint_passes(0, B, 0, adj, g)
+    r.cast_rays(0, pass_idx=0)
+
+    def timed(fn, n):
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / n
+
+    n = 2 * B
+    f1 = timed(lambda: [r.cast_rays(p % B, pass_idx=1000 + p) for p in range(n)], n)
+    fb = timed(lambda: [r.cast_rays_bundle(0, B, pass_idx=1000 + i * B) for i in range(2)], n)
+    ab = timed(lambda: r.adjoint_passes(0, n, 1000, adj, g), n)
+    bits = r.check_device()
+    r.close()
+    return {"workload": "inverse-rendering scene: box + 20k-tri HG medium (g 0.7) + fluorescent wall, 256x256, "
+                        "depth 32, 25 bands; parameters " + str(pm + pe),
+            "forward_ms_per_pass": f1, "forward_bundle_ms_per_pass": fb, "adjoint_ms_per_pass": ab,
+            "adjoint_over_forward": ab / f1, "adjoint_over_forward_bundle": ab / fb, "device_error_bits": bits}
+
+
+def bench_batch(args):
+    """Batched workload: scenes of seeds 100.. (box / terrain / volume, 1k-500k
+    triangles, 128^2-512^2, depth 4-16), each rendered to a relative XYZ RMSE
+    target, one scene at a time with one launch per pass (plain) and all
+    scenes together by the batched persistent kernel replayed as a CUDA graph."""
+    import torch
+    import spectral_b200 as sb
+    from spectral_b200 import batch as sbatch
+    from spectral_b200 import configs
+    t0 = time.time()
+    rs = []
+    for sc, cf, ex in configs.batch_workload(100, args.batch_scenes):
+        cf.kernel = "mega"
+        rs.append(sb.Renderer(sc, cf, eems=ex["eems"], cmf=ex["cmf"]))
+    build_s = time.time() - t0
+    B = rs[0].config.bands
+    target = args.batch_target
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    plain = []
+    for r in rs:
+        r.clear_pixel_space()
+        nb = 0
+        while True:
+            for k in range(B):
+                r.cast_rays(k, pass_idx=nb * B + k)
+            nb += 1
+            r.average_and_reset_block(nb)
+            if nb >= 2 and sbatch.relative_rmse_estimate(r, nb) <= target:
+                break
+        plain.append(nb)
+    torch.cuda.synchronize()
+    tp = time.perf_counter() - t0
+    with sbatch.Batch(rs, use_graph=True) as b:
+        b.reset()
+        b.step()
+        b.reset()
+        blocks, tb = b.render_to_rmse(target=target)
+        bits = b.check()
+    paths = sum(int(n) * B * r.config.width * r.config.height for n, r in zip(blocks, rs))
+    line = {"metric": f"seconds to {target:.0%} relative XYZ RMSE, all scenes", "value": tb, "unit": "s",
+            "higher_is_better": False, "n_gpus": 1, "impl": "ours", "data": "synthetic (seeded procedural scenes)",
+            "config": {"workload": f"{len(rs)} scenes of seeds 100-{99 + len(rs)}: box / terrain / volume, "
+                                   "1k-500k triangles, 128^2-512^2, depth 4-16",
+                       "scene_build_seconds": build_s},
+            "plain_seconds": tp, "batched_seconds": tb, "speedup": tp / tb,
+            "blocks_plain": plain, "blocks_batched": [int(x) for x in blocks],
+            "batched_mpaths_per_s": paths / tb / 1e6, "device_error_bits": bits,
+            "scenes": [{"res": r.config.width, "tris": r.compiled.num_tris, "depth": r.config.max_path_length}
+                       for r in rs]}
+    for r in rs:
+        r.close()
+    print(json.dumps(line))
 
 
 def bench_reference(args):
@@ -321,6 +498,12 @@ def bench_ours(args):
             "gpu_launches": launches_per_step * args.steps,
             "clocks": clocks, "device_error_bits": bits}
 
+    line["vertices_per_s"] = value * 1e6 * work["vertices"] / work["paths"]
+    if rank == 0 and world == 1 and not args.no_extras:
+        line["rmse"] = [rmse_leg("box", 0.01, args.rmse_seconds, bundles=True),
+                        rmse_leg("box", 0.01, args.rmse_seconds, bundles=False),
+                        rmse_leg("terrain", 0.05, args.rmse_seconds, bundles=True)]
+        line["adjoint"] = adjoint_leg()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, n, dt, threads, st = cpu_oracle_rate(comp, bvh, scene, cfg, seconds=12.0)
         line["cpu_baseline"] = {"value": rate / 1e6, "unit": "Mpaths/s", "cores": threads, "kind": "port",
@@ -337,5 +520,7 @@ if __name__ == "__main__":
     a = parse()
     if a.impl == "reference":
         bench_reference(a)
+    elif a.workload == "batch":
+        bench_batch(a)
     else:
         bench_ours(a)

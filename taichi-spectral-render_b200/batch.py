@@ -132,4 +132,4 @@ def relative_rmse_estimate(renderer, nblocks):
     import torch
     xyz, xvar = xyz_mean_and_variance(renderer, nblocks)
     den = float(torch.sum(xyz * xyz))
-    return float(torch.sqrt(torch.sum(xvar))) / max(np.sqrt(den), 1e-300)
+    return float(torch.sqrt(torch.sum(xvar))) / max(float(np.sqrt(den)), 1e-300)
