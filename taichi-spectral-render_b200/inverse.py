@@ -1,0 +1,129 @@
+"""Inverse rendering of spectral material parameters (the differentiable workload).
+
+The box scene with the HG medium and the fluorescent back wall, with 79
+unknowns: the per-band albedos of the left and right walls (2 x 25), the
+medium's per-band absorption sigma_a (25), its HG anisotropy g, and three
+GGX roughnesses (medium boundary, left wall, right wall).  A target image is
+rendered from hidden parameters, and Adam fits the parameters from an
+initial guess by minimising the L2 distance of the XYZ images, each step a
+forward render and a path-replay adjoint of the same paths
+(autodiff.render_film).
+
+Parameters live in an unconstrained space (albedo = sigmoid, sigma_a = exp,
+g = 0.95 tanh, roughness = sigmoid) and are mapped onto the material table
+[M][6][B] with torch operations, so autograd composes the mapping with the
+adjoint's table gradient.
+"""
+import math
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import autodiff
+from .configs import volume_scene
+
+LEFT, RIGHT, MEDIUM = 5, 6, 8  # material ids of volume_scene (walls 1..6, light 7, medium 8)
+
+
+@dataclass
+class Params:
+    albedo_left: torch.Tensor   # [B] in (0, 1)
+    albedo_right: torch.Tensor  # [B]
+    sigma_a: torch.Tensor       # [B] 1/m
+    g: torch.Tensor             # scalar in (-0.95, 0.95)
+    roughness: torch.Tensor     # [3]: medium boundary, left, right
+
+    @staticmethod
+    def from_scene_params(p, device):
+        f = lambda x: torch.as_tensor(np.asarray(x, np.float64), device=device)
+        return Params(f(p["albedo_left"]), f(p["albedo_right"]), f(p["sigma_a"]), f(p["g"]), f(p["roughness"]))
+
+    def count(self):
+        return sum(int(np.prod(t.shape)) if t.dim() else 1 for t in (self.albedo_left, self.albedo_right,
+                                                                      self.sigma_a, self.g, self.roughness))
+
+
+def to_unconstrained(p):
+    logit = lambda x: torch.log(x.clamp(1e-4, 1 - 1e-4)) - torch.log1p(-x.clamp(1e-4, 1 - 1e-4))
+    return [logit(p.albedo_left), logit(p.albedo_right), torch.log(p.sigma_a.clamp_min(1e-6)),
+            torch.atanh((p.g / 0.95).clamp(-0.999, 0.999)), logit(p.roughness)]
+
+
+def from_unconstrained(u):
+    return Params(torch.sigmoid(u[0]), torch.sigmoid(u[1]), torch.exp(u[2]), 0.95 * torch.tanh(u[3]),
+                  torch.sigmoid(u[4]))
+
+
+def material_table(base, p, wavelengths_nm):
+    """The material table [M][6][B] with the parameters written in (differentiable)."""
+    lam = torch.as_tensor(np.asarray(wavelengths_nm, np.float64) * 1e-9, device=base.device)
+    mat = base.to(torch.float64).clone()
+    k_of_albedo = lambda rho: lam * (1.0 / rho - 1.0) / (4.0 * math.pi)  # sigma_s = 1 gives albedo rho
+    mat[LEFT, 1] = k_of_albedo(p.albedo_left)
+    mat[RIGHT, 1] = k_of_albedo(p.albedo_right)
+    mat[MEDIUM, 1] = p.sigma_a * lam / (4.0 * math.pi)
+    mat[MEDIUM, 5] = p.g * torch.ones_like(lam)
+    mat[MEDIUM, 2] = p.roughness[0] * torch.ones_like(lam)
+    mat[LEFT, 2] = p.roughness[1] * torch.ones_like(lam)
+    mat[RIGHT, 2] = p.roughness[2] * torch.ones_like(lam)
+    return mat
+
+
+def scene_params(seed):
+    """79 parameters drawn from ``seed``: the wall albedos and sigma_a(lambda) as the
+    scene generator draws them for that seed (logistic reflectances, sums of two
+    Gaussians), g uniform in [0.3, 0.9] and roughnesses uniform in [0.05, 0.5]."""
+    _, _, ex = volume_scene(seed=seed, width=8, height=8, medium_slices=8, medium_stacks=9)
+    p = dict(ex["params"])
+    rng = np.random.default_rng(seed + 10_000)
+    p["g"] = float(rng.uniform(0.3, 0.9))
+    p["roughness"] = rng.uniform(0.05, 0.5, size=3).tolist()
+    return p
+
+
+def run(renderer, target_xyz, init, iterations=200, lr=1e-2, blocks=2, first_pass=1 << 20, log=None):
+    """Adam on the unconstrained parameters; returns the fitted Params and the loss history.
+
+    Each iteration renders ``blocks`` spectral blocks (new random streams per
+    iteration) and back-propagates through the same paths."""
+    r = renderer
+    base = autodiff.material_table(r)
+    eem = autodiff.eem_table(r)
+    lam = r.config.wavelengths()
+    u = [t.detach().clone().requires_grad_(True) for t in to_unconstrained(init)]
+    opt = torch.optim.Adam(u, lr=lr)
+    hist = []
+    B = r.config.bands
+    for it in range(iterations):
+        opt.zero_grad()
+        p = from_unconstrained(u)
+        mat = material_table(base, p, lam)
+        film = autodiff.render_film(r, mat, eem, first_pass=first_pass + it * blocks * B, num_blocks=blocks)
+        xyz = autodiff.film_to_xyz(film, r.compiled.cmf, r.cmf_scale)
+        loss = ((xyz - target_xyz) ** 2).mean()
+        loss.backward()
+        opt.step()
+        hist.append(float(loss))
+        if log is not None:
+            log(it, float(loss), p)
+    return from_unconstrained([t.detach() for t in u]), hist
+
+
+def render_target(renderer, params, blocks):
+    """XYZ image of ``params`` at ``blocks`` spectral blocks (no gradient)."""
+    r = renderer
+    base = autodiff.material_table(r)
+    mat = material_table(base, params, r.config.wavelengths()).float()
+    with torch.no_grad():
+        film = autodiff.render_film(r, mat, autodiff.eem_table(r), first_pass=0, num_blocks=blocks)
+        return autodiff.film_to_xyz(film, r.compiled.cmf, r.cmf_scale)
+
+
+def parameter_error(p, q):
+    """Relative L2 error of each parameter group of p against q."""
+    out = {}
+    for name in ("albedo_left", "albedo_right", "sigma_a", "g", "roughness"):
+        a, b = getattr(p, name), getattr(q, name)
+        out[name] = float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b).clamp_min(1e-12))
+    return out
