@@ -2,8 +2,11 @@
 
 The box scene with the HG medium and the fluorescent back wall, with 79
 unknowns: the per-band albedos of the left and right walls (2 x 25), the
-medium's per-band absorption sigma_a (25), its HG anisotropy g, and three
-GGX roughnesses (medium boundary, left wall, right wall).  A target image is
+medium's per-band absorption sigma_a (25), its HG anisotropy g, and the GGX
+roughnesses of the fluorescent back wall and the left and right walls (3).
+The medium's boundary stays a smooth dielectric: under the reference's
+estimator a rough dielectric boundary transmits nothing (its Smith term
+clamps the refracted cosine to zero), which would hide the medium.  A target image is
 rendered from hidden parameters, and Adam fits the parameters from an
 initial guess by minimising the L2 distance of the XYZ images, each step a
 forward render and a path-replay adjoint of the same paths
@@ -23,7 +26,7 @@ import torch
 from . import autodiff
 from .configs import volume_scene
 
-LEFT, RIGHT, MEDIUM = 5, 6, 8  # material ids of volume_scene (walls 1..6, light 7, medium 8)
+BACK, LEFT, RIGHT, MEDIUM = 3, 5, 6, 8  # material ids of volume_scene (walls 1..6, light 7, medium 8)
 
 
 @dataclass
@@ -32,7 +35,7 @@ class Params:
     albedo_right: torch.Tensor  # [B]
     sigma_a: torch.Tensor       # [B] 1/m
     g: torch.Tensor             # scalar in (-0.95, 0.95)
-    roughness: torch.Tensor     # [3]: medium boundary, left, right
+    roughness: torch.Tensor     # [3]: back, left, right wall
 
     @staticmethod
     def from_scene_params(p, device):
@@ -64,7 +67,7 @@ def material_table(base, p, wavelengths_nm):
     mat[RIGHT, 1] = k_of_albedo(p.albedo_right)
     mat[MEDIUM, 1] = p.sigma_a * lam / (4.0 * math.pi)
     mat[MEDIUM, 5] = p.g * torch.ones_like(lam)
-    mat[MEDIUM, 2] = p.roughness[0] * torch.ones_like(lam)
+    mat[BACK, 2] = p.roughness[0] * torch.ones_like(lam)
     mat[LEFT, 2] = p.roughness[1] * torch.ones_like(lam)
     mat[RIGHT, 2] = p.roughness[2] * torch.ones_like(lam)
     return mat
