@@ -107,9 +107,9 @@ def run(renderer, target_xyz, init, iterations=200, lr=1e-2, blocks=2, first_pas
         loss = ((xyz - target_xyz) ** 2).mean()
         loss.backward()
         opt.step()
-        hist.append(float(loss))
+        hist.append(float(loss.detach()))
         if log is not None:
-            log(it, float(loss), p)
+            log(it, hist[-1], p)
     return from_unconstrained([t.detach() for t in u]), hist
 
 
@@ -121,6 +121,16 @@ def render_target(renderer, params, blocks):
     with torch.no_grad():
         film = autodiff.render_film(r, mat, autodiff.eem_table(r), first_pass=0, num_blocks=blocks)
         return autodiff.film_to_xyz(film, r.compiled.cmf, r.cmf_scale)
+
+
+def image_loss(renderer, params, target_xyz, blocks=2, first_pass=1 << 20):
+    """The loss of ``run`` at fixed parameters (e.g. the hidden ones: the noise floor)."""
+    r = renderer
+    mat = material_table(autodiff.material_table(r), params, r.config.wavelengths()).float()
+    with torch.no_grad():
+        film = autodiff.render_film(r, mat, autodiff.eem_table(r), first_pass=first_pass, num_blocks=blocks)
+        xyz = autodiff.film_to_xyz(film, r.compiled.cmf, r.cmf_scale)
+        return float(((xyz - target_xyz) ** 2).mean())
 
 
 def parameter_error(p, q):

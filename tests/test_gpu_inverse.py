@@ -1,4 +1,4 @@
-"""Inverse rendering through the adjoint: Adam recovers perturbed parameters."""
+"""Inverse rendering through the adjoint: Adam lowers the image loss and recovers g."""
 import pytest
 import torch
 
@@ -24,6 +24,6 @@ def test_adam_reduces_image_loss_and_parameter_error():
         e1 = inverse.parameter_error(fit, hidden)
         assert all(torch.isfinite(torch.tensor(hist)))
         assert sum(hist[-5:]) < 0.5 * sum(hist[:5]), hist
-        assert e1["sigma_a"] < 0.7 * e0["sigma_a"], (e0, e1)
-        assert e1["g"] < 0.7 * e0["g"], (e0, e1)
+        # g is identifiable from the XYZ image; 25-band spectra are not (metamerism)
+        assert e1["g"] < 0.5 * e0["g"], (e0, e1)
         assert r.check_device() == 0
