@@ -102,6 +102,11 @@ typedef struct {
 /* ---- context (replaces ti.init + the module-global fields, main.py:9, 361-394) */
 ts_status ts_create(const ts_config *cfg, ts_ctx **out);
 ts_status ts_destroy(ts_ctx *ctx);
+/* Change the launch settings of a context -- kernel, traversal, block_size,
+ * blocks_per_sm, sort_keys, trace_budget of *cfg; every other field is
+ * ignored -- without re-uploading the scene (the autotuner's knob).  Paths and
+ * images do not depend on these settings. */
+ts_status ts_set_launch_config(ts_ctx *ctx, const ts_config *cfg);
 const char *ts_last_error(const ts_ctx *ctx); /* ctx may be NULL: last error of this thread */
 const char *ts_version(void);
 

@@ -63,6 +63,7 @@ _VP = ctypes.c_void_p
 SIGNATURES = [
     ("ts_create", ctypes.c_int, [ctypes.POINTER(TsConfig), ctypes.POINTER(_VP)]),
     ("ts_destroy", ctypes.c_int, [_VP]),
+    ("ts_set_launch_config", ctypes.c_int, [_VP, ctypes.POINTER(TsConfig)]),
     ("ts_last_error", ctypes.c_char_p, [_VP]),
     ("ts_version", ctypes.c_char_p, []),
     ("ts_upload_scene", ctypes.c_int, [_VP, ctypes.POINTER(TsSceneDesc)]),

@@ -1,0 +1,142 @@
+"""Autotuner: picks the launch configuration of a scene by timing candidates.
+
+Every candidate renders exactly the same paths (the random streams depend
+only on seed, pass, pixel and draw index), so tuning never changes an image,
+only its cost.  Knobs:
+
+  * BVH node width 2 / 4 / 8 (the scene is re-uploaded per width; the host
+    builder's tree is reused),
+  * traversal loop of two-child nodes (default if-if / speculative while-while),
+  * kernel: the persistent megakernel or the wavefront stages, and for the
+    wavefront its queue sorting (sort_keys bit mask) and the traversal steps
+    between lane refills (trace_budget),
+  * threads per block and resident blocks per SM of the persistent grid.
+
+Each candidate renders ``passes`` passes after ``warmup`` (CUDA events on the
+current stream); the fastest wins.  Results are cached in a JSON file keyed by
+a signature of the scene (triangles, materials, resolution, depth, bands).
+
+    best, table = tune(scene, cfg, eems=ex["eems"], cmf=ex["cmf"], cache="tune.json")
+    r = Renderer(scene, best.apply(cfg), eems=..., cmf=..., bvh_params={"width": best.width})
+"""
+import dataclasses
+import hashlib
+import json
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from .renderer import Renderer
+from .scene import compile_scene
+
+
+@dataclass(frozen=True)
+class Candidate:
+    width: int = 2
+    traversal: str = "default"
+    kernel: str = "mega"
+    block_size: int = 128
+    blocks_per_sm: int = 0
+    sort_keys: int = 0
+    trace_budget: int = 0
+
+    def apply(self, cfg):
+        """A copy of cfg with this candidate's launch settings."""
+        return dataclasses.replace(cfg, traversal=self.traversal, kernel=self.kernel, block_size=self.block_size,
+                                   blocks_per_sm=self.blocks_per_sm, sort_keys=self.sort_keys,
+                                   trace_budget=self.trace_budget)
+
+
+def default_candidates(quick=False):
+    out = [Candidate(w, "default", "mega", bs, bpsm) for w in (2, 4, 8) for bs in (64, 128) for bpsm in (0, 5)]
+    out += [Candidate(2, "speculative", "mega", 128, 0)]
+    if not quick:
+        out += [Candidate(w, "default", "wavefront", 128, 0, sk, tb)
+                for w in (2, 4) for sk in (0, 1) for tb in (16, 32, 64)]
+    return out
+
+
+def signature(compiled, cfg):
+    h = hashlib.sha1()
+    for a in (compiled.tris["v0"], compiled.mat_f32, compiled.mat_i32):
+        h.update(np.ascontiguousarray(a).tobytes())
+    h.update(repr((cfg.width, cfg.height, cfg.bands, cfg.max_path_length, cfg.scatter_bounces)).encode())
+    return h.hexdigest()[:16]
+
+
+def _time_passes(r, passes, warmup, first_pass):
+    import torch
+    B = r.config.bands
+    for p in range(warmup):
+        r.cast_rays(p % B, pass_idx=first_pass + p)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for p in range(passes):
+        r.cast_rays((warmup + p) % B, pass_idx=first_pass + warmup + p)
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / passes
+
+
+def tune(scene_dict, cfg, eems=None, cmf=None, candidates=None, passes=6, warmup=2, cache=None, quick=False,
+         first_pass=1 << 24):
+    """Time every candidate on this scene; returns (best Candidate, [(Candidate, ms per pass)])."""
+    compiled = compile_scene(scene_dict, cfg.bands, eems=eems, cmf=cmf)
+    key = signature(compiled, cfg)
+    if cache and os.path.exists(cache):
+        stored = json.load(open(cache)).get(key)
+        if stored:
+            best = Candidate(**stored["best"])
+            return best, [(Candidate(**c), ms) for c, ms in stored["table"]]
+    bvh = _lib.build_bvh_host(compiled.tris["v0"], compiled.tris["v1"], compiled.tris["v2"])
+    candidates = list(candidates or default_candidates(quick))
+    table = []
+    for width in sorted({c.width for c in candidates}):
+        group = [c for c in candidates if c.width == width]
+        with Renderer(scene_dict, group[0].apply(cfg), eems=eems, cmf=cmf, bvh=bvh,
+                      bvh_params={"width": width}) as r:
+            for cand in group:
+                r.set_launch_config(kernel=cand.kernel, traversal=cand.traversal, block_size=cand.block_size,
+                                    blocks_per_sm=cand.blocks_per_sm, sort_keys=cand.sort_keys,
+                                    trace_budget=cand.trace_budget)
+                ms = _time_passes(r, passes, warmup, first_pass)
+                if r.check_device() != 0:
+                    ms = float("inf")
+                table.append((cand, ms))
+    best = min(table, key=lambda t: t[1])[0]
+    if cache:
+        data = json.load(open(cache)) if os.path.exists(cache) else {}
+        data[key] = {"best": dataclasses.asdict(best), "table": [(dataclasses.asdict(c), ms) for c, ms in table]}
+        with open(cache, "w") as f:
+            json.dump(data, f, indent=1)
+    return best, table
+
+
+def tune_batch(renderers, block_sizes=(64, 128), blocks_per_sm=(3, 4, 5, 8), steps=2):
+    """Threads per block and resident blocks per SM of the batched kernel, timed
+    on ``steps`` steps of the given scenes (their BVH width is theirs; the films
+    are cleared afterwards).  Returns ((block_size, blocks_per_sm), [(setting, ms per step)])."""
+    import torch
+    from .batch import Batch
+    table = []
+    for bs in block_sizes:
+        for bpsm in blocks_per_sm:
+            with Batch(renderers, block_size=bs, blocks_per_sm=bpsm, use_graph=False) as b:
+                b.reset(first_pass=1 << 24)
+                b.step()
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                for _ in range(steps):
+                    b.step()
+                e1.record()
+                torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1) / steps
+                if b.check() != 0:
+                    ms = float("inf")
+                b.reset()
+            table.append(((bs, bpsm), ms))
+    return min(table, key=lambda t: t[1])[0], table

@@ -187,6 +187,24 @@ ts_status ts_create(const ts_config *cfg, ts_ctx **out) {
   return TS_OK;
 }
 
+ts_status ts_set_launch_config(ts_ctx *c, const ts_config *k) {
+  if (!c || !k) return fail(c, TS_ERR_INVALID_ARG, "ts_set_launch_config: null argument");
+  if (k->kernel != TS_KERNEL_MEGA && k->kernel != TS_KERNEL_WAVEFRONT)
+    return fail(c, TS_ERR_INVALID_ARG, "ts_set_launch_config: unknown kernel");
+  if (k->traversal != TS_TRAVERSAL_DEFAULT && k->traversal != TS_TRAVERSAL_SPECULATIVE)
+    return fail(c, TS_ERR_INVALID_ARG, "ts_set_launch_config: unknown traversal variant");
+  if (k->blocks_per_sm < 0 || k->blocks_per_sm > 64 || k->sort_keys < 0 || k->sort_keys > 7 || k->trace_budget < 0)
+    return fail(c, TS_ERR_INVALID_ARG, "ts_set_launch_config: launch parameter out of range");
+  c->cfg.kernel = k->kernel;
+  c->cfg.traversal = k->traversal;
+  c->cfg.block_size = std::min(ts::kMaxBlock, std::max(32, (k->block_size > 0 ? k->block_size : 128) / 32 * 32));
+  c->cfg.blocks_per_sm = k->blocks_per_sm;
+  c->cfg.sort_keys = k->sort_keys;
+  c->cfg.trace_budget = k->trace_budget > 0 ? k->trace_budget : 32;
+  c->dc.speculative = k->traversal == TS_TRAVERSAL_SPECULATIVE ? 1 : 0;
+  return TS_OK;
+}
+
 ts_status ts_destroy(ts_ctx *c) {
   if (!c) return TS_OK;
   cudaSetDevice(c->cfg.device);

@@ -19,6 +19,7 @@ film and scene buffers and takes the current torch stream).  Nothing here
 computes on the CPU: every render call is a CUDA launch through the C ABI.
 """
 import ctypes
+import dataclasses
 from dataclasses import dataclass
 
 import numpy as np
@@ -137,6 +138,16 @@ class Renderer:
 
     def _check(self, status):
         _lib.check(status, self._ctx)
+
+    def set_launch_config(self, kernel=None, traversal=None, block_size=None, blocks_per_sm=None, sort_keys=None,
+                          trace_budget=None):
+        """Change launch settings without re-uploading the scene (images do not depend on them)."""
+        upd = {k: v for k, v in dict(kernel=kernel, traversal=traversal, block_size=block_size,
+                                     blocks_per_sm=blocks_per_sm, sort_keys=sort_keys,
+                                     trace_budget=trace_budget).items() if v is not None}
+        cfg = dataclasses.replace(self.config, **upd)
+        self._check(self.lib.ts_set_launch_config(self._ctx, ctypes.byref(cfg.to_c())))
+        self.config = cfg
 
     # ---------------------------------------------------------------- scene
     def setup_scene(self, scene_dict, eems=None, cmf=None, bvh=None, bvh_params=None, exact=None):
