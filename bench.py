@@ -46,6 +46,8 @@ def parse():
     p.add_argument("--budget", type=int, default=0, help="wavefront traversal steps between refills")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-extras", action="store_true", help="skip the time-to-RMSE and adjoint-cost legs")
+    p.add_argument("--no-tune", action="store_true", help="use --kernel/--width/--traversal as given instead of "
+                                                          "the autotuner's choice")
     p.add_argument("--rmse-seconds", type=float, default=60.0, help="time limit of each time-to-RMSE leg")
     p.add_argument("--batch-scenes", type=int, default=64, help="scenes of the batched workload (--workload batch)")
     p.add_argument("--batch-target", type=float, default=0.05, help="RMSE target of the batched workload")
@@ -140,13 +142,13 @@ def measured_peak():
     return 6650.0, "of fallback"
 
 
-def profiled_traffic(kernel, workload_name):
+def profiled_traffic(kernel, workload_name, width):
     """DRAM bytes per launch from the committed ncu summary (None if not captured)."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
     if not os.path.exists(path):
         return None
     d = json.load(open(path))
-    e = d.get(f"{workload_name}:{kernel}")
+    e = d.get(f"{workload_name}:{kernel}:w{width}")
     return None if e is None else float(e["dram_bytes_per_launch"])
 
 
@@ -413,6 +415,21 @@ def bench_ours(args):
     cfg.traversal = args.traversal
     cfg.trace_budget = args.budget
     cfg.device = local
+    tuned = None
+    if not args.no_tune:
+        # launch configuration chosen by the autotuner (megakernel candidates: BVH width,
+        # traversal loop, block shape); every candidate renders the same paths
+        from spectral_b200 import autotune
+        t0 = time.time()
+        best, table = autotune.tune(scene, cfg, eems=ex["eems"], cmf=ex["cmf"], quick=True, passes=6,
+                                    first_pass=1 << 26)
+        cfg = best.apply(cfg)
+        args.width, args.kernel, args.traversal = best.width, best.kernel, best.traversal
+        tuned = {"seconds": time.time() - t0, "candidates": len(table),
+                 "best": {"width": best.width, "traversal": best.traversal, "kernel": best.kernel,
+                          "block_size": best.block_size, "blocks_per_sm": best.blocks_per_sm},
+                 "ms_per_pass": {f"w{c.width}/{c.traversal}/{c.kernel}/b{c.block_size}/s{c.blocks_per_sm}": round(ms, 4)
+                                 for c, ms in table}}
     comp = sb.compile_scene(scene, cfg.bands, eems=ex["eems"], cmf=ex["cmf"])
     bvh = sb._lib.build_bvh_host(comp.tris["v0"], comp.tris["v1"], comp.tris["v2"])
     r = sb.Renderer(scene, cfg, eems=ex["eems"], cmf=ex["cmf"], bvh=bvh, bvh_params={"width": args.width})
@@ -477,7 +494,7 @@ def bench_ours(args):
     peak, peak_src = measured_peak()
     step_s = ms_max * 1e-3 / args.steps
     achieved = bytes_per_path * paths_per_step / step_s / 1e9
-    traffic = profiled_traffic(args.kernel, args.workload)
+    traffic = profiled_traffic(args.kernel, args.workload, args.width)
 
     line = {"metric": "Mpaths/s", "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -499,7 +516,7 @@ def bench_ours(args):
                          "kernel": "k_render_mega" if args.kernel == "mega" else "wavefront pass",
                          "bytes_per_path": bytes_per_path, "peak_source": peak_src,
                          "work_per_path": {k: v / work["paths"] for k, v in work.items() if k != "paths"}},
-            "gpu_launches": launches_per_step * args.steps,
+            "gpu_launches": launches_per_step * args.steps, "autotune": tuned,
             "clocks": clocks, "device_error_bits": bits}
 
     line["vertices_per_s"] = value * 1e6 * work["vertices"] / work["paths"]
