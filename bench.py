@@ -331,7 +331,11 @@ def bench_batch(args):
         plain.append(nb)
     torch.cuda.synchronize()
     tp = time.perf_counter() - t0
-    with sbatch.Batch(rs, use_graph=True) as b:
+    from spectral_b200 import autotune
+    t0 = time.time()
+    (bs, bpsm, occ), _ = autotune.tune_batch(rs, steps=1)
+    tune_s = time.time() - t0
+    with sbatch.Batch(rs, block_size=bs, blocks_per_sm=bpsm, occupancy=occ, use_graph=True) as b:
         b.reset()
         b.step()
         b.reset()
@@ -344,6 +348,7 @@ def bench_batch(args):
                                    "1k-500k triangles, 128^2-512^2, depth 4-16",
                        "scene_build_seconds": build_s},
             "plain_seconds": tp, "batched_seconds": tb, "speedup": tp / tb,
+            "batch_autotune": {"block_size": bs, "blocks_per_sm": bpsm, "occupancy": occ, "seconds": tune_s},
             "blocks_plain": plain, "blocks_batched": [int(x) for x in blocks],
             "batched_mpaths_per_s": paths / tb / 1e6, "device_error_bits": bits,
             "scenes": [{"res": r.config.width, "tris": r.compiled.num_tris, "depth": r.config.max_path_length}
@@ -427,9 +432,10 @@ def bench_ours(args):
         args.width, args.kernel, args.traversal = best.width, best.kernel, best.traversal
         tuned = {"seconds": time.time() - t0, "candidates": len(table),
                  "best": {"width": best.width, "traversal": best.traversal, "kernel": best.kernel,
-                          "block_size": best.block_size, "blocks_per_sm": best.blocks_per_sm},
-                 "ms_per_pass": {f"w{c.width}/{c.traversal}/{c.kernel}/b{c.block_size}/s{c.blocks_per_sm}": round(ms, 4)
-                                 for c, ms in table}}
+                          "block_size": best.block_size, "blocks_per_sm": best.blocks_per_sm,
+                          "occupancy": best.occupancy},
+                 "ms_per_pass": {f"w{c.width}/{c.traversal}/{c.kernel}/b{c.block_size}/s{c.blocks_per_sm}"
+                                 f"/o{c.occupancy}": round(ms, 4) for c, ms in table}}
     comp = sb.compile_scene(scene, cfg.bands, eems=ex["eems"], cmf=ex["cmf"])
     bvh = sb._lib.build_bvh_host(comp.tris["v0"], comp.tris["v1"], comp.tris["v2"])
     r = sb.Renderer(scene, cfg, eems=ex["eems"], cmf=ex["cmf"], bvh=bvh, bvh_params={"width": args.width})

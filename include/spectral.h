@@ -61,6 +61,8 @@ typedef struct {
                                     2 extension rays by direction octant, 4 shadow rays by light (0 = off) */
   int32_t trace_budget;          /* wavefront: traversal steps between refills of idle lanes (0 = 32) */
   int32_t traversal;             /* TS_TRAVERSAL_DEFAULT or TS_TRAVERSAL_SPECULATIVE (two-child nodes) */
+  int32_t occupancy;             /* megakernel register budget: 0 = 5 resident blocks of 128 per SM (96 registers),
+                                    8 = 8 blocks (64 registers, spills; more latency hiding on large frames) */
 } ts_config;
 
 /* Scene in the reference's data model (setup_scene, main.py:509-631). Triangles
@@ -103,7 +105,7 @@ typedef struct {
 ts_status ts_create(const ts_config *cfg, ts_ctx **out);
 ts_status ts_destroy(ts_ctx *ctx);
 /* Change the launch settings of a context -- kernel, traversal, block_size,
- * blocks_per_sm, sort_keys, trace_budget of *cfg; every other field is
+ * blocks_per_sm, sort_keys, trace_budget, occupancy of *cfg; every other field is
  * ignored -- without re-uploading the scene (the autotuner's knob).  Paths and
  * images do not depend on these settings. */
 ts_status ts_set_launch_config(ts_ctx *ctx, const ts_config *cfg);
@@ -234,6 +236,7 @@ typedef struct {
   int32_t block_size;     /* render-kernel threads per block, 32..128 (0 = 128) */
   int32_t blocks_per_sm;  /* persistent grid = SMs * blocks_per_sm (0 = 5) */
   int32_t use_graph;      /* 1: capture the step's four kernels as one CUDA graph at the first step, replay after */
+  int32_t occupancy;      /* 0 = 5 resident blocks per SM (96 registers), 8 = 8 blocks (64 registers) */
 } ts_batch_config;
 
 ts_status ts_batch_create(const ts_batch_config *cfg, ts_ctx *const *ctxs, int32_t num_scenes, ts_batch **out);

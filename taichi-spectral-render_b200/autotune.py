@@ -10,7 +10,8 @@ only its cost.  Knobs:
   * kernel: the persistent megakernel or the wavefront stages, and for the
     wavefront its queue sorting (sort_keys bit mask) and the traversal steps
     between lane refills (trace_budget),
-  * threads per block and resident blocks per SM of the persistent grid.
+  * threads per block and resident blocks per SM of the persistent grid, and
+    the megakernel's register budget (5 blocks/SM without spills, or 8 with).
 
 Each candidate renders ``passes`` passes after ``warmup`` (CUDA events on the
 current stream); the fastest wins.  Results are cached in a JSON file keyed by
@@ -41,17 +42,19 @@ class Candidate:
     blocks_per_sm: int = 0
     sort_keys: int = 0
     trace_budget: int = 0
+    occupancy: int = 0
 
     def apply(self, cfg):
         """A copy of cfg with this candidate's launch settings."""
         return dataclasses.replace(cfg, traversal=self.traversal, kernel=self.kernel, block_size=self.block_size,
                                    blocks_per_sm=self.blocks_per_sm, sort_keys=self.sort_keys,
-                                   trace_budget=self.trace_budget)
+                                   trace_budget=self.trace_budget, occupancy=self.occupancy)
 
 
 def default_candidates(quick=False):
     out = [Candidate(w, "default", "mega", bs, bpsm) for w in (2, 4, 8) for bs in (64, 128) for bpsm in (0, 5)]
-    out += [Candidate(2, "speculative", "mega", 128, 0)]
+    out += [Candidate(w, "default", "mega", 128, 0, occupancy=8) for w in (2, 4, 8)]
+    out += [Candidate(2, "speculative", "mega", 128, 0), Candidate(2, "speculative", "mega", 128, 0, occupancy=8)]
     if not quick:
         out += [Candidate(w, "default", "wavefront", 128, 0, sk, tb)
                 for w in (2, 4) for sk in (0, 1) for tb in (16, 32, 64)]
@@ -101,7 +104,7 @@ def tune(scene_dict, cfg, eems=None, cmf=None, candidates=None, passes=6, warmup
             for cand in group:
                 r.set_launch_config(kernel=cand.kernel, traversal=cand.traversal, block_size=cand.block_size,
                                     blocks_per_sm=cand.blocks_per_sm, sort_keys=cand.sort_keys,
-                                    trace_budget=cand.trace_budget)
+                                    trace_budget=cand.trace_budget, occupancy=cand.occupancy)
                 ms = _time_passes(r, passes, warmup, first_pass)
                 if r.check_device() != 0:
                     ms = float("inf")
@@ -115,28 +118,28 @@ def tune(scene_dict, cfg, eems=None, cmf=None, candidates=None, passes=6, warmup
     return best, table
 
 
-def tune_batch(renderers, block_sizes=(64, 128), blocks_per_sm=(3, 4, 5, 8), steps=2):
-    """Threads per block and resident blocks per SM of the batched kernel, timed
-    on ``steps`` steps of the given scenes (their BVH width is theirs; the films
-    are cleared afterwards).  Returns ((block_size, blocks_per_sm), [(setting, ms per step)])."""
+def tune_batch(renderers, block_sizes=(64, 128), blocks_per_sm=(5, 8), occupancies=(0, 8), steps=2):
+    """Threads per block, blocks per SM of the persistent grid and register budget of
+    the batched kernel, timed on ``steps`` steps of the given scenes (their BVH
+    width is theirs; the films are cleared afterwards).
+    Returns ((block_size, blocks_per_sm, occupancy), [(setting, ms per step)])."""
     import torch
     from .batch import Batch
     table = []
-    for bs in block_sizes:
-        for bpsm in blocks_per_sm:
-            with Batch(renderers, block_size=bs, blocks_per_sm=bpsm, use_graph=False) as b:
-                b.reset(first_pass=1 << 24)
+    for bs, bpsm, occ in [(a, b, c) for a in block_sizes for b in blocks_per_sm for c in occupancies]:
+        with Batch(renderers, block_size=bs, blocks_per_sm=bpsm, use_graph=False, occupancy=occ) as b:
+            b.reset(first_pass=1 << 24)
+            b.step()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(steps):
                 b.step()
-                torch.cuda.synchronize()
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record()
-                for _ in range(steps):
-                    b.step()
-                e1.record()
-                torch.cuda.synchronize()
-                ms = e0.elapsed_time(e1) / steps
-                if b.check() != 0:
-                    ms = float("inf")
-                b.reset()
-            table.append(((bs, bpsm), ms))
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / steps
+            if b.check() != 0:
+                ms = float("inf")
+            b.reset()
+        table.append(((bs, bpsm, occ), ms))
     return min(table, key=lambda t: t[1])[0], table

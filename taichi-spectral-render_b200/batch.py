@@ -21,7 +21,8 @@ from .renderer import _stream
 
 
 class TsBatchConfig(ctypes.Structure):
-    _fields_ = [("block_size", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32), ("use_graph", ctypes.c_int32)]
+    _fields_ = [("block_size", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32), ("use_graph", ctypes.c_int32),
+                ("occupancy", ctypes.c_int32)]
 
 
 def _check(lib, status, handle):
@@ -33,12 +34,12 @@ def _check(lib, status, handle):
 class Batch:
     """Scenes (Renderer objects on one device, one BVH width) rendered together."""
 
-    def __init__(self, renderers, block_size=0, blocks_per_sm=0, use_graph=True):
+    def __init__(self, renderers, block_size=0, blocks_per_sm=0, use_graph=True, occupancy=0):
         self.renderers = list(renderers)
         self.lib = _lib.load()
         n = len(self.renderers)
         arr = (ctypes.c_void_p * n)(*[r._ctx.value for r in self.renderers])
-        cfg = TsBatchConfig(int(block_size), int(blocks_per_sm), 1 if use_graph else 0)
+        cfg = TsBatchConfig(int(block_size), int(blocks_per_sm), 1 if use_graph else 0, int(occupancy))
         self._h = ctypes.c_void_p()
         _check(self.lib, self.lib.ts_batch_create(ctypes.byref(cfg), arr, n, ctypes.byref(self._h)), None)
         self.active = np.ones(n, bool)

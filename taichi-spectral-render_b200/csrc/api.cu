@@ -136,6 +136,8 @@ ts_status ts_create(const ts_config *cfg, ts_ctx **out) {
     return fail(nullptr, TS_ERR_INVALID_ARG, "ts_create: unknown kernel");
   if (k.traversal != TS_TRAVERSAL_DEFAULT && k.traversal != TS_TRAVERSAL_SPECULATIVE)
     return fail(nullptr, TS_ERR_INVALID_ARG, "ts_create: unknown traversal variant");
+  if (k.occupancy != 0 && k.occupancy != 5 && k.occupancy != 8)
+    return fail(nullptr, TS_ERR_INVALID_ARG, "ts_create: occupancy must be 0, 5 or 8");
   int ndev = 0;
   cudaError_t e = cudaGetDeviceCount(&ndev);
   if (e != cudaSuccess || ndev == 0) return fail(nullptr, TS_ERR_CUDA, "ts_create: no CUDA device");
@@ -200,7 +202,10 @@ ts_status ts_set_launch_config(ts_ctx *c, const ts_config *k) {
   c->cfg.block_size = std::min(ts::kMaxBlock, std::max(32, (k->block_size > 0 ? k->block_size : 128) / 32 * 32));
   c->cfg.blocks_per_sm = k->blocks_per_sm;
   c->cfg.sort_keys = k->sort_keys;
+  if (k->occupancy != 0 && k->occupancy != 5 && k->occupancy != 8)
+    return fail(c, TS_ERR_INVALID_ARG, "ts_set_launch_config: occupancy must be 0, 5 or 8");
   c->cfg.trace_budget = k->trace_budget > 0 ? k->trace_budget : 32;
+  c->cfg.occupancy = k->occupancy;
   c->dc.speculative = k->traversal == TS_TRAVERSAL_SPECULATIVE ? 1 : 0;
   return TS_OK;
 }
@@ -484,7 +489,8 @@ ts_status ts_render_pass(ts_ctx *c, uint32_t pass_idx, int32_t band, void *strea
     int per_sm = c->cfg.blocks_per_sm;
     if (per_sm <= 0) per_sm = std::max(1, 2048 / bs);
     const int grid = c->num_sms * per_sm;
-    TS_CUDA(c, ts::launch_render_mega(c->ds, c->dc, pass_idx, band, film_of(c), c->d_counter, c->d_err, grid, bs, st),
+    TS_CUDA(c, ts::launch_render_mega(c->ds, c->dc, pass_idx, band, film_of(c), c->d_counter, c->d_err, grid, bs, st,
+                                      nullptr, 1, c->cfg.occupancy),
             "render pass");
   } else {
     ts_status s = ensure_wave(c);
@@ -520,7 +526,7 @@ ts_status ts_render_passes(ts_ctx *c, uint32_t first_pass, int32_t num_passes, i
   int per_sm = c->cfg.blocks_per_sm;
   if (per_sm <= 0) per_sm = std::max(1, 2048 / bs);
   TS_CUDA(c, ts::launch_render_mega(c->ds, c->dc, first_pass, first_band, film_of(c), c->d_counter, c->d_err,
-                                    c->num_sms * per_sm, bs, as_stream(stream), nullptr, num_passes),
+                                    c->num_sms * per_sm, bs, as_stream(stream), nullptr, num_passes, c->cfg.occupancy),
           "ts_render_passes");
   return TS_OK;
 }
@@ -885,14 +891,14 @@ ts_status ts_batch_step(ts_batch *b, void *stream) {
   const int acc_blocks = b->num_sms * 2;
   if (!b->cfg.use_graph) {
     TS_BCUDA(b, ts::launch_batch_step(b->d_slots, b->n, b->d_hdr, b->d_active, b->d_err, b->width, grid,
-                                      b->cfg.block_size, acc_blocks, as_stream(stream)),
+                                      b->cfg.block_size, acc_blocks, as_stream(stream), b->cfg.occupancy),
              "ts_batch_step");
     return TS_OK;
   }
   if (!b->exec) {
     TS_BCUDA(b, cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal), "ts_batch_step: capture");
     const cudaError_t le = ts::launch_batch_step(b->d_slots, b->n, b->d_hdr, b->d_active, b->d_err, b->width, grid,
-                                                 b->cfg.block_size, acc_blocks, b->cap);
+                                                 b->cfg.block_size, acc_blocks, b->cap, b->cfg.occupancy);
     const cudaError_t ce = cudaStreamEndCapture(b->cap, &b->graph);
     TS_BCUDA(b, le, "ts_batch_step: capture");
     TS_BCUDA(b, ce, "ts_batch_step: capture");

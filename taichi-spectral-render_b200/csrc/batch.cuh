@@ -31,6 +31,6 @@ size_t batch_smem_bytes(int n);
 cudaError_t batch_set_smem_limit(int n);
 // one step: prepare (item ranges), render (persistent pool), accumulate, advance
 cudaError_t launch_batch_step(BatchSlot *slots, int n, BatchHeader *h, const int *active, uint32_t *err, int width,
-                              int grid, int block, int acc_blocks, cudaStream_t st);
+                              int grid, int block, int acc_blocks, cudaStream_t st, int occupancy);
 
 }  // namespace ts

@@ -21,7 +21,7 @@ struct Film {
 // work != nullptr selects the counting variant (work[8], accumulated)
 cudaError_t launch_render_mega(const DevScene &s, const DevConfig &c, uint32_t pass, int band, Film f,
                                int *counter, uint32_t *err, int grid, int block, cudaStream_t st,
-                               unsigned long long *work = nullptr, int npass = 1);
+                               unsigned long long *work = nullptr, int npass = 1, int occupancy = 0);
 
 // closest hit for a ray batch; mode 0 = fast traversal, 1 = reference order
 cudaError_t launch_trace_batch(const DevScene &s, float eps, const float *rays, int n, int mode, int32_t *tri_orig,

@@ -45,8 +45,8 @@ __device__ __forceinline__ int find_slot(const BatchSlot *sh, int n, int idx) {
   return lo;
 }
 
-template <int W>
-__global__ void __launch_bounds__(128, 5) k_render_batch(const BatchSlot *__restrict__ slots, int n,
+template <int W, int kMinBlocks = 5>
+__global__ void __launch_bounds__(128, kMinBlocks) k_render_batch(const BatchSlot *__restrict__ slots, int n,
                                                       BatchHeader *__restrict__ h, uint32_t *__restrict__ err) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   BatchSlot *sh = reinterpret_cast<BatchSlot *>(smem_raw);
@@ -125,15 +125,24 @@ __global__ void k_batch_advance(BatchSlot *slots, int n) {
 
 size_t batch_smem_bytes(int n) { return (size_t)n * sizeof(BatchSlot); }
 
+namespace {
+template <int kMin>
+void launch_render_batch(BatchSlot *slots, int n, BatchHeader *h, uint32_t *err, int width, int grid, int block,
+                         size_t smem, cudaStream_t st) {
+  if (width == 8) k_render_batch<8, kMin><<<grid, block, smem, st>>>(slots, n, h, err);
+  else if (width == 4) k_render_batch<4, kMin><<<grid, block, smem, st>>>(slots, n, h, err);
+  else if (width == 3) k_render_batch<3, kMin><<<grid, block, smem, st>>>(slots, n, h, err);
+  else k_render_batch<2, kMin><<<grid, block, smem, st>>>(slots, n, h, err);
+}
+}  // namespace
+
 cudaError_t launch_batch_step(BatchSlot *slots, int n, BatchHeader *h, const int *active, uint32_t *err, int width,
-                              int grid, int block, int acc_blocks, cudaStream_t st) {
+                              int grid, int block, int acc_blocks, cudaStream_t st, int occupancy) {
   k_batch_prepare<<<1, 32, 0, st>>>(slots, n, h, active);
   const size_t smem = batch_smem_bytes(n);
   block = block > 128 ? 128 : block;
-  if (width == 8) k_render_batch<8><<<grid, block, smem, st>>>(slots, n, h, err);
-  else if (width == 4) k_render_batch<4><<<grid, block, smem, st>>>(slots, n, h, err);
-  else if (width == 3) k_render_batch<3><<<grid, block, smem, st>>>(slots, n, h, err);
-  else k_render_batch<2><<<grid, block, smem, st>>>(slots, n, h, err);
+  if (occupancy >= 8) launch_render_batch<8>(slots, n, h, err, width, grid, block, smem, st);
+  else launch_render_batch<5>(slots, n, h, err, width, grid, block, smem, st);
   k_batch_accumulate<<<dim3(acc_blocks, n), 256, 0, st>>>(slots);
   k_batch_advance<<<(n + 127) / 128, 128, 0, st>>>(slots, n);
   return cudaGetLastError();
@@ -142,10 +151,15 @@ cudaError_t launch_batch_step(BatchSlot *slots, int n, BatchHeader *h, const int
 cudaError_t batch_set_smem_limit(int n) {
   const int bytes = (int)batch_smem_bytes(n);
   cudaError_t e = cudaSuccess;
-  for (cudaError_t r : {cudaFuncSetAttribute(k_render_batch<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
-                        cudaFuncSetAttribute(k_render_batch<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
-                        cudaFuncSetAttribute(k_render_batch<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
-                        cudaFuncSetAttribute(k_render_batch<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)})
+  for (cudaError_t r :
+       {cudaFuncSetAttribute(k_render_batch<2, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
+        cudaFuncSetAttribute(k_render_batch<3, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
+        cudaFuncSetAttribute(k_render_batch<4, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
+        cudaFuncSetAttribute(k_render_batch<8, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
+        cudaFuncSetAttribute(k_render_batch<2, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
+        cudaFuncSetAttribute(k_render_batch<3, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
+        cudaFuncSetAttribute(k_render_batch<4, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
+        cudaFuncSetAttribute(k_render_batch<8, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)})
     if (r != cudaSuccess) e = r;
   return e;
 }

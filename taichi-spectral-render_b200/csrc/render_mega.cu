@@ -18,8 +18,11 @@ namespace {
 // kCount: also count the work (for the roofline's algorithmic bytes):
 // work[0..7] = paths, path vertices, traversals, node visits, triangle tests,
 // surface hits resolved, film deposits, (unused).
-template <int W, bool kCount>
-__global__ void __launch_bounds__(128, 5) k_render_mega(DevScene s, DevConfig c, uint32_t pass0, int npass, int band0,
+// kMinBlocks: resident blocks of 128 threads per SM the compiler must allow
+// (5: 96 registers, no spills; 8: 64 registers with local-memory spills --
+// more warps to hide the node-fetch latency, faster on large frames).
+template <int W, bool kCount, int kMinBlocks = 5>
+__global__ void __launch_bounds__(128, kMinBlocks) k_render_mega(DevScene s, DevConfig c, uint32_t pass0, int npass, int band0,
                                                      Film f, int *__restrict__ counter, uint32_t *__restrict__ err,
                                                      unsigned long long *__restrict__ work) {
   const int lane = threadIdx.x & 31;
@@ -69,8 +72,10 @@ __global__ void __launch_bounds__(128, 5) k_render_mega(DevScene s, DevConfig c,
 
 template <int W>
 void launch_w(const DevScene &s, const DevConfig &c, uint32_t pass0, int npass, int band0, Film f, int *counter,
-              uint32_t *err, int grid, int block, cudaStream_t st, unsigned long long *work) {
+              uint32_t *err, int grid, int block, cudaStream_t st, unsigned long long *work, int occupancy) {
   if (work) k_render_mega<W, true><<<grid, block, 0, st>>>(s, c, pass0, npass, band0, f, counter, err, work);
+  else if (occupancy >= 8)
+    k_render_mega<W, false, 8><<<grid, block, 0, st>>>(s, c, pass0, npass, band0, f, counter, err, nullptr);
   else k_render_mega<W, false><<<grid, block, 0, st>>>(s, c, pass0, npass, band0, f, counter, err, nullptr);
 }
 
@@ -78,14 +83,14 @@ void launch_w(const DevScene &s, const DevConfig &c, uint32_t pass0, int npass, 
 
 cudaError_t launch_render_mega(const DevScene &s, const DevConfig &c, uint32_t pass, int band, Film f,
                                int *counter, uint32_t *err, int grid, int block, cudaStream_t st,
-                               unsigned long long *work, int npass) {
+                               unsigned long long *work, int npass, int occupancy) {
   cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), st);
   if (e != cudaSuccess) return e;
   block = block > 128 ? 128 : block;  // the kernel is compiled for blocks of at most 128 threads
-  if (s.node_width == 8) launch_w<8>(s, c, pass, npass, band, f, counter, err, grid, block, st, work);
-  else if (s.node_width == 4) launch_w<4>(s, c, pass, npass, band, f, counter, err, grid, block, st, work);
-  else if (c.speculative) launch_w<3>(s, c, pass, npass, band, f, counter, err, grid, block, st, work);
-  else launch_w<2>(s, c, pass, npass, band, f, counter, err, grid, block, st, work);
+  if (s.node_width == 8) launch_w<8>(s, c, pass, npass, band, f, counter, err, grid, block, st, work, occupancy);
+  else if (s.node_width == 4) launch_w<4>(s, c, pass, npass, band, f, counter, err, grid, block, st, work, occupancy);
+  else if (c.speculative) launch_w<3>(s, c, pass, npass, band, f, counter, err, grid, block, st, work, occupancy);
+  else launch_w<2>(s, c, pass, npass, band, f, counter, err, grid, block, st, work, occupancy);
   return cudaGetLastError();
 }
 
