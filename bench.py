@@ -198,9 +198,14 @@ def rmse_leg(name, target, seconds, bundles=True):
     import torch
     import spectral_b200 as sb
     from spectral_b200 import batch as sbatch
+    from spectral_b200 import autotune
     scene, cfg, ex, desc = workload(name)
-    cfg.kernel = "mega"
-    r = sb.Renderer(scene, cfg, eems=ex["eems"], cmf=ex["cmf"])
+    # megakernel launch settings from the autotuner (bundles need the megakernel)
+    cands = [c for c in autotune.default_candidates(quick=True) if c.kernel == "mega"]
+    best, _ = autotune.tune(scene, cfg, eems=ex["eems"], cmf=ex["cmf"], candidates=cands, passes=4,
+                            first_pass=1 << 26)
+    cfg = best.apply(cfg)
+    r = sb.Renderer(scene, cfg, eems=ex["eems"], cmf=ex["cmf"], bvh_params={"width": best.width})
     B = cfg.bands
     r.cast_rays_bundle(0, B, pass_idx=0)
     r.clear_pixel_space()
@@ -228,6 +233,8 @@ def rmse_leg(name, target, seconds, bundles=True):
     secs = time.perf_counter() - t0
     est = sbatch.relative_rmse_estimate(r, nb)
     out = {"workload": name, "target": target, "blocks": nb, "spp": nb * B, "seconds": secs,
+           "launch": {"width": best.width, "traversal": best.traversal, "block_size": best.block_size,
+                      "blocks_per_sm": best.blocks_per_sm, "occupancy": best.occupancy},
            "estimated_rmse": float(est), "reached": bool(est <= target),
            "launches": "one per block (wavelength bundle)" if bundles else "one per pass"}
     if est > target:
