@@ -43,6 +43,7 @@ def parse():
     p.add_argument("--workload", default="terrain", choices=["terrain", "box", "volume", "batch"])
     p.add_argument("--width", type=int, default=2, choices=[2, 4, 8], help="BVH node width")
     p.add_argument("--traversal", default="default", choices=["default", "speculative"])
+    p.add_argument("--occupancy", type=int, default=0, choices=[0, 8], help="megakernel register budget (--no-tune)")
     p.add_argument("--budget", type=int, default=0, help="wavefront traversal steps between refills")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-extras", action="store_true", help="skip the time-to-RMSE and adjoint-cost legs")
@@ -142,13 +143,13 @@ def measured_peak():
     return 6650.0, "of fallback"
 
 
-def profiled_traffic(kernel, workload_name, width):
+def profiled_traffic(kernel, workload_name, width, occupancy):
     """DRAM bytes per launch from the committed ncu summary (None if not captured)."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
     if not os.path.exists(path):
         return None
     d = json.load(open(path))
-    e = d.get(f"{workload_name}:{kernel}:w{width}")
+    e = d.get(f"{workload_name}:{kernel}:w{width}" + (f":o{occupancy}" if occupancy else ""))
     return None if e is None else float(e["dram_bytes_per_launch"])
 
 
@@ -426,6 +427,7 @@ def bench_ours(args):
     cfg.kernel = args.kernel
     cfg.traversal = args.traversal
     cfg.trace_budget = args.budget
+    cfg.occupancy = args.occupancy
     cfg.device = local
     tuned = None
     if not args.no_tune:
@@ -436,7 +438,7 @@ def bench_ours(args):
         best, table = autotune.tune(scene, cfg, eems=ex["eems"], cmf=ex["cmf"], quick=True, passes=6,
                                     first_pass=1 << 26)
         cfg = best.apply(cfg)
-        args.width, args.kernel, args.traversal = best.width, best.kernel, best.traversal
+        args.width, args.kernel, args.traversal, args.occupancy = best.width, best.kernel, best.traversal, best.occupancy
         tuned = {"seconds": time.time() - t0, "candidates": len(table),
                  "best": {"width": best.width, "traversal": best.traversal, "kernel": best.kernel,
                           "block_size": best.block_size, "blocks_per_sm": best.blocks_per_sm,
@@ -507,13 +509,14 @@ def bench_ours(args):
     peak, peak_src = measured_peak()
     step_s = ms_max * 1e-3 / args.steps
     achieved = bytes_per_path * paths_per_step / step_s / 1e9
-    traffic = profiled_traffic(args.kernel, args.workload, args.width)
+    traffic = profiled_traffic(args.kernel, args.workload, args.width, args.occupancy)
 
     line = {"metric": "Mpaths/s", "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded procedural scene; no dataset)",
             "config": {"workload": desc, "kernel": args.kernel, "bvh_width": args.width, "traversal": args.traversal,
+                       "occupancy": args.occupancy,
                        "paths_per_step": paths_per_step,
                        "spp": ex["spp"], "passes_for_spp": cfg.samples_per_pixel,
                        "l2": "inputs larger than L2: scene %.0f MB + film %.0f MB > 126 MB L2; no flush"
