@@ -42,3 +42,19 @@ def reduce_film(mean, m2, num_blocks, group=None):
         mean.div_(total)
     dist.all_reduce(m2, group=group)
     return mean, m2, int(round(total))
+
+
+def adjoint_range(total_passes, rank, world):
+    """Contiguous share [first, last) of ``total_passes`` adjoint passes for ``rank``
+    (the adjoint has no film planes, so passes need not come in whole blocks)."""
+    return block_range(total_passes, rank, world)
+
+
+def reduce_gradient(grad, group=None):
+    """Sum the per-rank FP64 parameter gradients (each rank replayed its own passes)
+    in place on every rank: the one exchange of a multi-GPU adjoint."""
+    import torch.distributed as dist
+    if grad.dtype != torch.float64:
+        raise TypeError("gradients are reduced in float64")
+    dist.all_reduce(grad, group=group)
+    return grad

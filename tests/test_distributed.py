@@ -63,3 +63,35 @@ def test_reduce_film_gloo_world2():
         assert total == allb.shape[0]
         assert np.allclose(mean, allb.mean(0), rtol=1e-13)
         assert np.allclose(m2, (allb ** 2).sum(0), rtol=1e-13)
+
+
+def _grad_worker(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    first, last = sd.adjoint_range(7, rank, world)
+    # each rank's partial gradient: a stand-in sum over its own passes
+    g = torch.zeros(79, dtype=torch.float64)
+    for p in range(first, last):
+        g += torch.from_numpy(np.random.default_rng(p).normal(size=79))
+    sd.reduce_gradient(g)
+    q.put((rank, g.numpy()))
+    dist.destroy_process_group()
+
+
+def test_reduce_gradient_gloo_world2():
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_grad_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=120) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    want = sum(np.random.default_rng(p).normal(size=79) for p in range(7))
+    for _, g in res:
+        assert np.allclose(g, want, rtol=1e-13, atol=1e-13)
+    with pytest.raises(TypeError):
+        sd.reduce_gradient(torch.zeros(3, dtype=torch.float32))
