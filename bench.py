@@ -539,7 +539,8 @@ def bench_ours(args):
     if rank == 0 and world == 1 and not args.no_extras:
         line["rmse"] = [rmse_leg("box", 0.01, args.rmse_seconds, bundles=True),
                         rmse_leg("box", 0.01, args.rmse_seconds, bundles=False),
-                        rmse_leg("terrain", 0.05, args.rmse_seconds, bundles=True)]
+                        rmse_leg("terrain", 0.05, args.rmse_seconds, bundles=True),
+                        rmse_leg("volume", 0.05, args.rmse_seconds, bundles=True)]
         line["adjoint"] = adjoint_leg()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, n, dt, threads, st = cpu_oracle_rate(comp, bvh, scene, cfg, seconds=12.0)
