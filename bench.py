@@ -203,8 +203,8 @@ def rmse_leg(name, target, seconds, bundles=True):
     scene, cfg, ex, desc = workload(name)
     # megakernel launch settings from the autotuner (bundles need the megakernel)
     cands = [c for c in autotune.default_candidates(quick=True) if c.kernel == "mega"]
-    best, _ = autotune.tune(scene, cfg, eems=ex["eems"], cmf=ex["cmf"], candidates=cands, passes=4,
-                            first_pass=1 << 26)
+    best, _ = autotune.tune(scene, cfg, eems=ex["eems"], cmf=ex["cmf"], candidates=cands, passes=50 if bundles else 6,
+                            first_pass=1 << 26, bundles=bundles)
     cfg = best.apply(cfg)
     r = sb.Renderer(scene, cfg, eems=ex["eems"], cmf=ex["cmf"], bvh_params={"width": best.width})
     B = cfg.bands

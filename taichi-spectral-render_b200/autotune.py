@@ -61,17 +61,30 @@ def default_candidates(quick=False):
     return out
 
 
-def signature(compiled, cfg):
+def signature(compiled, cfg, bundles=False):
     h = hashlib.sha1()
     for a in (compiled.tris["v0"], compiled.mat_f32, compiled.mat_i32):
         h.update(np.ascontiguousarray(a).tobytes())
     h.update(repr((cfg.width, cfg.height, cfg.bands, cfg.max_path_length, cfg.scatter_bounces)).encode())
+    h.update(b"bundles" if bundles else b"passes")
     return h.hexdigest()[:16]
 
 
-def _time_passes(r, passes, warmup, first_pass):
+def _time_passes(r, passes, warmup, first_pass, bundles=False):
+    """ms per pass: one launch per pass, or one launch per block (bundles)."""
     import torch
     B = r.config.bands
+    if bundles:
+        r.cast_rays_bundle(0, B, pass_idx=first_pass)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        blocks = max(1, passes // B)
+        a.record()
+        for k in range(blocks):
+            r.cast_rays_bundle(0, B, pass_idx=first_pass + (k + 1) * B)
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / (blocks * B)
     for p in range(warmup):
         r.cast_rays(p % B, pass_idx=first_pass + p)
     torch.cuda.synchronize()
@@ -85,10 +98,13 @@ def _time_passes(r, passes, warmup, first_pass):
 
 
 def tune(scene_dict, cfg, eems=None, cmf=None, candidates=None, passes=6, warmup=2, cache=None, quick=False,
-         first_pass=1 << 24):
-    """Time every candidate on this scene; returns (best Candidate, [(Candidate, ms per pass)])."""
+         first_pass=1 << 24, bundles=False):
+    """Time every candidate on this scene; returns (best Candidate, [(Candidate, ms per pass)]).
+
+    bundles: time whole-block launches (cast_rays_bundle, megakernel candidates only)
+    instead of one launch per pass -- the two favour different block shapes."""
     compiled = compile_scene(scene_dict, cfg.bands, eems=eems, cmf=cmf)
-    key = signature(compiled, cfg)
+    key = signature(compiled, cfg, bundles)
     if cache and os.path.exists(cache):
         stored = json.load(open(cache)).get(key)
         if stored:
@@ -96,6 +112,8 @@ def tune(scene_dict, cfg, eems=None, cmf=None, candidates=None, passes=6, warmup
             return best, [(Candidate(**c), ms) for c, ms in stored["table"]]
     bvh = _lib.build_bvh_host(compiled.tris["v0"], compiled.tris["v1"], compiled.tris["v2"])
     candidates = list(candidates or default_candidates(quick))
+    if bundles:
+        candidates = [c for c in candidates if c.kernel == "mega"]
     table = []
     for width in sorted({c.width for c in candidates}):
         group = [c for c in candidates if c.width == width]
@@ -105,7 +123,7 @@ def tune(scene_dict, cfg, eems=None, cmf=None, candidates=None, passes=6, warmup
                 r.set_launch_config(kernel=cand.kernel, traversal=cand.traversal, block_size=cand.block_size,
                                     blocks_per_sm=cand.blocks_per_sm, sort_keys=cand.sort_keys,
                                     trace_budget=cand.trace_budget, occupancy=cand.occupancy)
-                ms = _time_passes(r, passes, warmup, first_pass)
+                ms = _time_passes(r, passes, warmup, first_pass, bundles)
                 if r.check_device() != 0:
                     ms = float("inf")
                 table.append((cand, ms))
