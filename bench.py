@@ -537,6 +537,23 @@ def bench_ours(args):
 
     line["vertices_per_s"] = value * 1e6 * work["vertices"] / work["paths"]
     if rank == 0 and world == 1 and not args.no_extras:
+        # the plain single-scene wavefront kernel on the same workload (same paths)
+        r.set_launch_config(kernel="wavefront", traversal="default", block_size=128, blocks_per_sm=0, sort_keys=0,
+                            trace_budget=16, occupancy=0)
+        for k in range(3):
+            r.cast_rays(k % B, pass_idx=base_pass + 9000 + k)
+        torch.cuda.synchronize()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        nw = max(10, args.steps // 10)
+        g0.record()
+        for k in range(nw):
+            r.cast_rays(k % B, pass_idx=base_pass + 9100 + k)
+        g1.record()
+        torch.cuda.synchronize()
+        wms = g0.elapsed_time(g1) / nw
+        line["plain_wavefront"] = {"value": paths_per_step / (wms * 1e-3) / 1e6, "unit": "Mpaths/s",
+                                   "ms_per_step": wms, "bvh_width": args.width, "trace_budget": 16}
+    if rank == 0 and world == 1 and not args.no_extras:
         line["rmse"] = [rmse_leg("box", 0.01, args.rmse_seconds, bundles=True),
                         rmse_leg("box", 0.01, args.rmse_seconds, bundles=False),
                         rmse_leg("terrain", 0.05, args.rmse_seconds, bundles=True),

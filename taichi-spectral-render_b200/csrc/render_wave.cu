@@ -165,8 +165,10 @@ void launch_trace(const DevScene &s, const DevConfig &c, int depth, Film f, cons
 
 // ---- queue sorting ------------------------------------------------------
 // Counting sorts that reorder a queue by a small key so that neighbouring
-// lanes of a warp take similar work: the shading queue by hit material, the
-// extension rays by direction octant, the shadow queries by light triangle.
+// lanes of a warp take similar work: the shading queue by (hit material,
+// medium the path travels in) -- by material alone when the pairs outnumber
+// the key table --, the extension rays by direction octant, the shadow queries
+// by light triangle.
 // Each is count (block histograms) -> scan -> scatter (one atomic per key per
 // warp, lanes of equal keys grouped with __match_any_sync).
 enum SortKind { kSortShade = 0, kSortExt = 1, kSortShadow = 2 };
@@ -183,8 +185,10 @@ __device__ __forceinline__ int sort_item(const WaveBuffers &w, int kind, int dep
 __device__ __forceinline__ int sort_key(const DevScene &s, const WaveBuffers &w, int kind, int item, int nkeys) {
   int key;
   if (kind == kSortShade) {
+    const int M = s.num_materials;
     const int slot = __float_as_int(w.hit[item].w);
-    key = slot >= 0 ? __float_as_int(__ldg(s.tri + 3 * (size_t)slot + 1).w) : s.num_materials;
+    key = slot >= 0 ? __float_as_int(__ldg(s.tri + 3 * (size_t)slot + 1).w) : M;
+    if ((M + 1) * M <= nkeys) key = key * M + w.meta[item].z;  // (material, medium)
   } else if (kind == kSortExt) {
     const float4 d = w.dir_spdf[item];
     key = (d.x < 0.f ? 1 : 0) | (d.y < 0.f ? 2 : 0) | (d.z < 0.f ? 4 : 0);
@@ -345,7 +349,8 @@ cudaError_t launch_wave_pass(const DevScene &s, const DevConfig &c, uint32_t pas
   k_generate<<<gen_grid, 256, 0, st>>>(s, c, pass, band, w);
   // sort_keys bit 0: shading queue by material; bit 1: extension rays by
   // direction octant; bit 2: shadow queries by light triangle
-  const int nmat = s.num_materials + 1 < kMaxKeys ? s.num_materials + 1 : kMaxKeys;
+  const int M = s.num_materials;
+  const int nmat = (M + 1) * M <= kMaxKeys ? (M + 1) * M : (M + 1 < kMaxKeys ? M + 1 : kMaxKeys);
   if (sort_keys) {
     e = cudaMemsetAsync(w.key_hist, 0, 2 * kMaxKeys * sizeof(int), st);
     if (e != cudaSuccess) return e;
