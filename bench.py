@@ -40,7 +40,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=10)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--kernel", default="mega", choices=["mega", "wavefront"])
-    p.add_argument("--workload", default="terrain", choices=["terrain", "box", "volume", "batch"])
+    p.add_argument("--workload", default="terrain", choices=["terrain", "box", "volume", "batch", "adjoint"])
     p.add_argument("--width", type=int, default=2, choices=[2, 4, 8], help="BVH node width")
     p.add_argument("--traversal", default="default", choices=["default", "speculative"])
     p.add_argument("--occupancy", type=int, default=0, choices=[0, 8], help="megakernel register budget (--no-tune)")
@@ -304,6 +304,40 @@ def adjoint_leg():
                         "depth 32, 25 bands; parameters " + str(pm + pe),
             "forward_ms_per_pass": f1, "forward_bundle_ms_per_pass": fb, "adjoint_ms_per_pass": ab,
             "adjoint_over_forward": ab / f1, "adjoint_over_forward_bundle": ab / fb, "device_error_bits": bits}
+
+
+def bench_adjoint(args):
+    """Path-replay adjoint on the inverse-rendering scene: --steps launches of one
+    block (25 passes) each after --warmup, CUDA events; prints one JSON line."""
+    import torch
+    import spectral_b200 as sb
+    from spectral_b200 import configs
+    s, c, ex = configs.volume_scene(width=256, height=256, depth=32)
+    c.kernel = "mega"
+    r = sb.Renderer(s, c, eems=ex["eems"], cmf=ex["cmf"])
+    B = c.bands
+    pm, pe = r.param_count()
+    adj = torch.rand((B, c.height, c.width), dtype=torch.float64, device="cuda")
+    g = torch.zeros(pm + pe, dtype=torch.float64, device="cuda")
+    for w in range(args.warmup):
+        r.adjoint_passes(0, B, w * B, adj, g)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for k in range(args.steps):
+        r.adjoint_passes(0, B, (args.warmup + k) * B, adj, g)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    bits = r.check_device()
+    r.close()
+    paths = B * c.width * c.height
+    print(json.dumps({"metric": "adjoint Mpaths/s", "value": paths / (ms * 1e-3) / 1e6, "unit": "Mpaths/s",
+                      "ms_per_step": ms, "steps": args.steps, "warmup": args.warmup, "n_gpus": 1,
+                      "higher_is_better": True, "data": "synthetic (seeded procedural scene)",
+                      "config": {"workload": "inverse-rendering scene 256x256, depth 32; one step = the adjoint of "
+                                             "one spectral block (25 passes)", "parameters": pm + pe},
+                      "device_error_bits": bits}))
 
 
 def bench_batch(args):
@@ -577,5 +611,7 @@ if __name__ == "__main__":
         bench_reference(a)
     elif a.workload == "batch":
         bench_batch(a)
+    elif a.workload == "adjoint":
+        bench_adjoint(a)
     else:
         bench_ours(a)
