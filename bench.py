@@ -52,6 +52,7 @@ def parse():
     p.add_argument("--rmse-seconds", type=float, default=60.0, help="time limit of each time-to-RMSE leg")
     p.add_argument("--batch-scenes", type=int, default=64, help="scenes of the batched workload (--workload batch)")
     p.add_argument("--batch-target", type=float, default=0.05, help="RMSE target of the batched workload")
+    p.add_argument("--passes", type=int, default=25, help="passes per adjoint launch (--workload adjoint)")
     return p.parse_args()
 
 
@@ -307,8 +308,8 @@ def adjoint_leg():
 
 
 def bench_adjoint(args):
-    """Path-replay adjoint on the inverse-rendering scene: --steps launches of one
-    block (25 passes) each after --warmup, CUDA events; prints one JSON line."""
+    """Path-replay adjoint on the inverse-rendering scene: --steps launches of
+    --passes passes each after --warmup, CUDA events; prints one JSON line."""
     import torch
     import spectral_b200 as sb
     from spectral_b200 import configs
@@ -319,24 +320,25 @@ def bench_adjoint(args):
     pm, pe = r.param_count()
     adj = torch.rand((B, c.height, c.width), dtype=torch.float64, device="cuda")
     g = torch.zeros(pm + pe, dtype=torch.float64, device="cuda")
+    P = args.passes
     for w in range(args.warmup):
-        r.adjoint_passes(0, B, w * B, adj, g)
+        r.adjoint_passes(0, P, w * P, adj, g)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for k in range(args.steps):
-        r.adjoint_passes(0, B, (args.warmup + k) * B, adj, g)
+        r.adjoint_passes(0, P, (args.warmup + k) * P, adj, g)
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
     bits = r.check_device()
     r.close()
-    paths = B * c.width * c.height
+    paths = P * c.width * c.height
     print(json.dumps({"metric": "adjoint Mpaths/s", "value": paths / (ms * 1e-3) / 1e6, "unit": "Mpaths/s",
                       "ms_per_step": ms, "steps": args.steps, "warmup": args.warmup, "n_gpus": 1,
                       "higher_is_better": True, "data": "synthetic (seeded procedural scene)",
-                      "config": {"workload": "inverse-rendering scene 256x256, depth 32; one step = the adjoint of "
-                                             "one spectral block (25 passes)", "parameters": pm + pe},
+                      "config": {"workload": f"inverse-rendering scene 256x256, depth 32; one step = the adjoint of "
+                                             f"{P} passes", "parameters": pm + pe},
                       "device_error_bits": bits}))
 
 
