@@ -364,14 +364,17 @@ def bench_batch(args):
     plain = []
     for r in rs:
         r.clear_pixel_space()
-        nb = 0
+        nb, due = 0, 2
         while True:
             for k in range(B):
                 r.cast_rays(k, pass_idx=nb * B + k)
             nb += 1
             r.average_and_reset_block(nb)
-            if nb >= 2 and sbatch.relative_rmse_estimate(r, nb) <= target:
-                break
+            if nb >= due:  # the same checking policy as Batch.render_to_rmse
+                e = sbatch.relative_rmse_estimate(r, nb)
+                if e <= target:
+                    break
+                due = sbatch.next_check(nb, e, target)
         plain.append(nb)
     torch.cuda.synchronize()
     tp = time.perf_counter() - t0

@@ -92,28 +92,40 @@ class Batch:
         _check(self.lib, self.lib.ts_batch_check(self._h, ctypes.byref(bits)), self._h)
         return bits.value
 
-    def render_to_rmse(self, target=0.01, max_blocks=100000, check_every=1, min_blocks=2, estimator=None):
+    def render_to_rmse(self, target=0.01, max_blocks=100000, min_blocks=2, estimator=None):
         """Steps until every scene's relative XYZ RMSE estimate is <= target.
 
-        Returns per-scene blocks rendered and the wall time (device-synchronised)."""
+        A scene's estimate is evaluated only when it is due: after an estimate e
+        at n blocks the next check comes at the block count where 1/sqrt(n)
+        scaling predicts the target (``next_check``).  Returns per-scene blocks
+        rendered and the wall time (device-synchronised)."""
         import torch
         estimator = estimator or relative_rmse_estimate
+        due = np.full(len(self.renderers), min_blocks, np.int64)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        steps = 0
         while self.active.any():
             self.step()
-            steps += 1
-            if steps % check_every == 0 or self.blocks.max() >= max_blocks:
-                flags = self.active.copy()
-                for i, r in enumerate(self.renderers):
-                    if flags[i] and self.blocks[i] >= min_blocks:
-                        if self.blocks[i] >= max_blocks or estimator(r, int(self.blocks[i])) <= target:
-                            flags[i] = False
-                if (flags != self.active).any():
-                    self.set_active(flags)
+            flags = self.active.copy()
+            for i, r in enumerate(self.renderers):
+                n = int(self.blocks[i])
+                if not flags[i] or (n < due[i] and n < max_blocks):
+                    continue
+                e = estimator(r, n)
+                if e <= target or n >= max_blocks:
+                    flags[i] = False
+                else:
+                    due[i] = next_check(n, e, target)
+            if (flags != self.active).any():
+                self.set_active(flags)
         torch.cuda.synchronize()
         return self.blocks.copy(), time.perf_counter() - t0
+
+
+def next_check(n, estimate, target):
+    """Block count at which to look again: where the estimate, falling as 1/sqrt(n),
+    is predicted to reach the target (90 % of the way, at most doubling n)."""
+    return n + max(1, min(n, int(n * ((estimate / target) ** 2 - 1) * 0.9)))
 
 
 def xyz_mean_and_variance(renderer, nblocks):
