@@ -230,7 +230,9 @@ ts_status ts_adjoint_passes(ts_ctx *ctx, uint32_t first_pass, int32_t num_passes
  * bands).  The batch
  * snapshots the contexts' scenes, cameras and films at creation: contexts must
  * outlive the batch and keep their scene uploaded.  All scenes must live on
- * one device and share the BVH width and traversal variant. */
+ * one device and share the BVH width and traversal variant.  Internally the
+ * work pool puts the deepest scenes first; arguments stay in the caller's
+ * scene order. */
 typedef struct ts_batch ts_batch;
 typedef struct {
   int32_t block_size;     /* render-kernel threads per block, 32..128 (0 = 128) */

@@ -752,7 +752,8 @@ struct ts_batch {
   int num_sms = 0;
   std::vector<ts_ctx *> ctxs;
   std::vector<ts::BatchSlot> host;
-  std::vector<int32_t> active;
+  std::vector<int32_t> active;  // per slot
+  std::vector<int> order;       // slot k renders the caller's scene order[k]
   ts::BatchSlot *d_slots = nullptr;
   ts::BatchHeader *d_hdr = nullptr;
   int *d_active = nullptr;
@@ -817,15 +818,25 @@ ts_status ts_batch_create(const ts_batch_config *cfg, ts_ctx *const *ctxs, int32
   if (b->cfg.blocks_per_sm <= 0) b->cfg.blocks_per_sm = 5;  // the render kernel's resident blocks per SM
   cudaSetDevice(b->device);
   cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, b->device);
-  b->ctxs.assign(ctxs, ctxs + n);
+  // Work-pool order: deepest scenes first (then larger frames), so that a
+  // step drains on the shortest paths instead of idling behind the longest.
+  b->order.resize(n);
+  for (int i = 0; i < n; ++i) b->order[i] = i;
+  std::stable_sort(b->order.begin(), b->order.end(), [&](int x, int y) {
+    const ts::DevConfig &a = ctxs[x]->dc, &c = ctxs[y]->dc;
+    if (a.max_depth != c.max_depth) return a.max_depth > c.max_depth;
+    return (int64_t)a.W * a.H > (int64_t)c.W * c.H;
+  });
+  b->ctxs.resize(n);
+  for (int k = 0; k < n; ++k) b->ctxs[k] = ctxs[b->order[k]];
   b->host.resize(n);
   b->active.assign(n, 1);
-  for (int i = 0; i < n; ++i) {
-    ts::BatchSlot &sl = b->host[i];
+  for (int k = 0; k < n; ++k) {
+    ts::BatchSlot &sl = b->host[k];
     std::memset(&sl, 0, sizeof(sl));
-    sl.s = ctxs[i]->ds;
-    sl.c = ctxs[i]->dc;
-    sl.f = film_of(ctxs[i]);
+    sl.s = b->ctxs[k]->ds;
+    sl.c = b->ctxs[k]->dc;
+    sl.f = film_of(b->ctxs[k]);
     sl.active = 1;
   }
   cudaError_t e = cudaMalloc((void **)&b->d_slots, sizeof(ts::BatchSlot) * n);
@@ -876,7 +887,7 @@ ts_status ts_batch_reset(ts_batch *b, uint32_t first_pass, void *stream) {
 ts_status ts_batch_set_active(ts_batch *b, const int32_t *active, void *stream) {
   if (!b || !active) return bfail(b, TS_ERR_INVALID_ARG, "ts_batch_set_active: null argument");
   cudaSetDevice(b->device);
-  for (int i = 0; i < b->n; ++i) b->active[i] = active[i] ? 1 : 0;
+  for (int k = 0; k < b->n; ++k) b->active[k] = active[b->order[k]] ? 1 : 0;
   TS_BCUDA(b, cudaMemcpyAsync(b->d_active, b->active.data(), sizeof(int) * b->n, cudaMemcpyHostToDevice,
                               as_stream(stream)),
            "ts_batch_set_active");
