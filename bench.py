@@ -44,6 +44,8 @@ def parse():
     p.add_argument("--width", type=int, default=2, choices=[2, 4, 8], help="BVH node width")
     p.add_argument("--traversal", default="default", choices=["default", "speculative"])
     p.add_argument("--occupancy", type=int, default=0, choices=[0, 8], help="megakernel register budget (--no-tune)")
+    p.add_argument("--launch", default="bundle", choices=["bundle", "pass"],
+                   help="render the timed passes 25 per launch (wavelength bundles) or one per launch")
     p.add_argument("--budget", type=int, default=0, help="wavefront traversal steps between refills")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-extras", action="store_true", help="skip the time-to-RMSE and adjoint-cost legs")
@@ -474,8 +476,9 @@ def bench_ours(args):
         # traversal loop, block shape); every candidate renders the same paths
         from spectral_b200 import autotune
         t0 = time.time()
-        best, table = autotune.tune(scene, cfg, eems=ex["eems"], cmf=ex["cmf"], quick=True, passes=6,
-                                    first_pass=1 << 26)
+        bundles = args.launch == "bundle"
+        best, table = autotune.tune(scene, cfg, eems=ex["eems"], cmf=ex["cmf"], quick=True,
+                                    passes=50 if bundles else 6, first_pass=1 << 26, bundles=bundles)
         cfg = best.apply(cfg)
         args.width, args.kernel, args.traversal, args.occupancy = best.width, best.kernel, best.traversal, best.occupancy
         tuned = {"seconds": time.time() - t0, "candidates": len(table),
@@ -508,9 +511,17 @@ def bench_ours(args):
     sampler.start()
     time.sleep(0.3)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    use_bundles = args.launch == "bundle" and args.kernel == "mega"
     e0.record()
-    for k in range(args.steps):
-        r.cast_rays(k % B, pass_idx=base_pass + args.warmup + 1 + k)
+    k = 0
+    while k < args.steps:  # exactly K passes; whole wavelength bundles when asked, single passes after
+        p0 = base_pass + args.warmup + 1 + k
+        if use_bundles and args.steps - k >= B:
+            r.cast_rays_bundle(k % B, B, pass_idx=p0)
+            k += B
+        else:
+            r.cast_rays(k % B, pass_idx=p0)
+            k += 1
     e1.record()
     torch.cuda.synchronize()
     clocks = sampler.stop()
@@ -545,6 +556,8 @@ def bench_ours(args):
     e2e_value = world * e2e_steps * paths_per_step / (float(t2.item()) * 1e-3) / 1e6
 
     launches_per_step = 1 if args.kernel == "mega" else 2 + 2 * cfg.max_path_length
+    if use_bundles:
+        launches_per_step = 1.0 / B
     peak, peak_src = measured_peak()
     step_s = ms_max * 1e-3 / args.steps
     achieved = bytes_per_path * paths_per_step / step_s / 1e9
@@ -556,6 +569,8 @@ def bench_ours(args):
             "data": "synthetic (seeded procedural scene; no dataset)",
             "config": {"workload": desc, "kernel": args.kernel, "bvh_width": args.width, "traversal": args.traversal,
                        "occupancy": args.occupancy,
+                       "launches": ("one launch per 25-pass wavelength bundle (each pass its own band, the same "
+                                    "paths as one launch per pass)" if use_bundles else "one launch per pass"),
                        "paths_per_step": paths_per_step,
                        "spp": ex["spp"], "passes_for_spp": cfg.samples_per_pixel,
                        "l2": "inputs larger than L2: scene %.0f MB + film %.0f MB > 126 MB L2; no flush"
@@ -571,10 +586,23 @@ def bench_ours(args):
                          "kernel": "k_render_mega" if args.kernel == "mega" else "wavefront pass",
                          "bytes_per_path": bytes_per_path, "peak_source": peak_src,
                          "work_per_path": {k: v / work["paths"] for k, v in work.items() if k != "paths"}},
-            "gpu_launches": launches_per_step * args.steps, "autotune": tuned,
+            "gpu_launches": int(round(launches_per_step * args.steps + (args.steps % B if use_bundles else 0))),
+            "autotune": tuned,
             "clocks": clocks, "device_error_bits": bits}
 
     line["vertices_per_s"] = value * 1e6 * work["vertices"] / work["paths"]
+    if use_bundles:
+        # the same passes with one launch per pass (the reference's cadence), for comparison
+        torch.cuda.synchronize()
+        h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        n1 = 2 * B
+        h0.record()
+        for k in range(n1):
+            r.cast_rays(k % B, pass_idx=base_pass + 8000 + k)
+        h1.record()
+        torch.cuda.synchronize()
+        line["one_launch_per_pass"] = {"value": paths_per_step / (h0.elapsed_time(h1) / n1 * 1e-3) / 1e6,
+                                       "unit": "Mpaths/s", "ms_per_pass": h0.elapsed_time(h1) / n1}
     if rank == 0 and world == 1 and not args.no_extras:
         # the plain single-scene wavefront kernel on the same workload (same paths)
         r.set_launch_config(kernel="wavefront", traversal="default", block_size=128, blocks_per_sm=0, sort_keys=0,
