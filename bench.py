@@ -583,6 +583,7 @@ def bench_ours(args):
                             "step, through the C ABI"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
+                         "traffic_per": "pass (ncu capture of a one-pass launch of the same configuration)",
                          "kernel": "k_render_mega" if args.kernel == "mega" else "wavefront pass",
                          "bytes_per_path": bytes_per_path, "peak_source": peak_src,
                          "work_per_path": {k: v / work["paths"] for k, v in work.items() if k != "paths"}},
