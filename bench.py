@@ -146,13 +146,14 @@ def measured_peak():
     return 6650.0, "of fallback"
 
 
-def profiled_traffic(kernel, workload_name, width, occupancy):
+def profiled_traffic(kernel, workload_name, width, occupancy, bundles=False):
     """DRAM bytes per launch from the committed ncu summary (None if not captured)."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
     if not os.path.exists(path):
         return None
     d = json.load(open(path))
-    e = d.get(f"{workload_name}:{kernel}:w{width}" + (f":o{occupancy}" if occupancy else ""))
+    e = d.get(f"{workload_name}:{kernel}:w{width}" + (f":o{occupancy}" if occupancy else "") +
+              (":bundle" if bundles else ""))
     return None if e is None else float(e["dram_bytes_per_launch"])
 
 
@@ -561,7 +562,7 @@ def bench_ours(args):
     peak, peak_src = measured_peak()
     step_s = ms_max * 1e-3 / args.steps
     achieved = bytes_per_path * paths_per_step / step_s / 1e9
-    traffic = profiled_traffic(args.kernel, args.workload, args.width, args.occupancy)
+    traffic = profiled_traffic(args.kernel, args.workload, args.width, args.occupancy, use_bundles)
 
     line = {"metric": "Mpaths/s", "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -583,7 +584,7 @@ def bench_ours(args):
                             "step, through the C ABI"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "traffic_per": "pass (ncu capture of a one-pass launch of the same configuration)",
+                         "traffic_per": "pass (ncu capture of a launch of the same configuration, per pass)",
                          "kernel": "k_render_mega" if args.kernel == "mega" else "wavefront pass",
                          "bytes_per_path": bytes_per_path, "peak_source": peak_src,
                          "work_per_path": {k: v / work["paths"] for k, v in work.items() if k != "paths"}},
