@@ -464,7 +464,8 @@ def bench_ours(args):
     torch.cuda.set_device(local)
     if world > 1:
         from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+        # bounded wait: ranks build their scene and tune before the first barrier
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
     scene, cfg, ex, desc = workload(args.workload)
     cfg.kernel = args.kernel
     cfg.traversal = args.traversal
