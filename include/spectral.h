@@ -63,6 +63,8 @@ typedef struct {
   int32_t traversal;             /* TS_TRAVERSAL_DEFAULT or TS_TRAVERSAL_SPECULATIVE (two-child nodes) */
   int32_t occupancy;             /* megakernel register budget: 0 = 5 resident blocks of 128 per SM (96 registers),
                                     8 = 8 blocks (64 registers, spills; more latency hiding on large frames) */
+  int32_t queue_capacity;        /* wavefront: paths per chunk of the frame (0 = whole frame); the queues and
+                                    path state of one chunk are allocated, so a small capacity keeps them in L2 */
 } ts_config;
 
 /* Scene in the reference's data model (setup_scene, main.py:509-631). Triangles
@@ -105,7 +107,7 @@ typedef struct {
 ts_status ts_create(const ts_config *cfg, ts_ctx **out);
 ts_status ts_destroy(ts_ctx *ctx);
 /* Change the launch settings of a context -- kernel, traversal, block_size,
- * blocks_per_sm, sort_keys, trace_budget, occupancy of *cfg; every other field is
+ * blocks_per_sm, sort_keys, trace_budget, occupancy, queue_capacity of *cfg; every other field is
  * ignored -- without re-uploading the scene (the autotuner's knob).  Paths and
  * images do not depend on these settings. */
 ts_status ts_set_launch_config(ts_ctx *ctx, const ts_config *cfg);

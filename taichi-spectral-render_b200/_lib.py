@@ -36,7 +36,8 @@ class TsConfig(ctypes.Structure):
                 ("fov_scale", ctypes.c_float), ("seed", ctypes.c_uint32), ("scene_id", ctypes.c_uint32),
                 ("device", ctypes.c_int32), ("kernel", ctypes.c_int32), ("block_size", ctypes.c_int32),
                 ("blocks_per_sm", ctypes.c_int32), ("sort_keys", ctypes.c_int32), ("trace_budget", ctypes.c_int32),
-                ("traversal", ctypes.c_int32), ("occupancy", ctypes.c_int32)]
+                ("traversal", ctypes.c_int32), ("occupancy", ctypes.c_int32),
+                ("queue_capacity", ctypes.c_int32)]
 
 
 class TsSceneDesc(ctypes.Structure):

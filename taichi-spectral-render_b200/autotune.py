@@ -8,8 +8,9 @@ only its cost.  Knobs:
     builder's tree is reused),
   * traversal loop of two-child nodes (default if-if / speculative while-while),
   * kernel: the persistent megakernel or the wavefront stages, and for the
-    wavefront its queue sorting (sort_keys bit mask) and the traversal steps
-    between lane refills (trace_budget),
+    wavefront its queue sorting (sort_keys bit mask), the traversal steps
+    between lane refills (trace_budget) and the queue capacity (paths per
+    chunk of the frame),
   * threads per block and resident blocks per SM of the persistent grid, and
     the megakernel's register budget (5 blocks/SM without spills, or 8 with).
 
@@ -43,12 +44,14 @@ class Candidate:
     sort_keys: int = 0
     trace_budget: int = 0
     occupancy: int = 0
+    queue_capacity: int = 0
 
     def apply(self, cfg):
         """A copy of cfg with this candidate's launch settings."""
         return dataclasses.replace(cfg, traversal=self.traversal, kernel=self.kernel, block_size=self.block_size,
                                    blocks_per_sm=self.blocks_per_sm, sort_keys=self.sort_keys,
-                                   trace_budget=self.trace_budget, occupancy=self.occupancy)
+                                   trace_budget=self.trace_budget, occupancy=self.occupancy,
+                                   queue_capacity=self.queue_capacity)
 
 
 def default_candidates(quick=False):
@@ -58,6 +61,8 @@ def default_candidates(quick=False):
     if not quick:
         out += [Candidate(w, "default", "wavefront", 128, 0, sk, tb)
                 for w in (2, 4) for sk in (0, 1) for tb in (16, 32, 64)]
+        out += [Candidate(w, "default", "wavefront", 128, 0, 0, 16, queue_capacity=qc)
+                for w in (2, 4) for qc in (1 << 16, 1 << 18)]
     return out
 
 
@@ -122,7 +127,8 @@ def tune(scene_dict, cfg, eems=None, cmf=None, candidates=None, passes=6, warmup
             for cand in group:
                 r.set_launch_config(kernel=cand.kernel, traversal=cand.traversal, block_size=cand.block_size,
                                     blocks_per_sm=cand.blocks_per_sm, sort_keys=cand.sort_keys,
-                                    trace_budget=cand.trace_budget, occupancy=cand.occupancy)
+                                    trace_budget=cand.trace_budget, occupancy=cand.occupancy,
+                                    queue_capacity=cand.queue_capacity)
                 ms = _time_passes(r, passes, warmup, first_pass, bundles)
                 if r.check_device() != 0:
                     ms = float("inf")

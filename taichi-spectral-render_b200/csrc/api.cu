@@ -138,6 +138,7 @@ ts_status ts_create(const ts_config *cfg, ts_ctx **out) {
     return fail(nullptr, TS_ERR_INVALID_ARG, "ts_create: unknown traversal variant");
   if (k.occupancy != 0 && k.occupancy != 5 && k.occupancy != 8)
     return fail(nullptr, TS_ERR_INVALID_ARG, "ts_create: occupancy must be 0, 5 or 8");
+  if (k.queue_capacity < 0) return fail(nullptr, TS_ERR_INVALID_ARG, "ts_create: negative queue_capacity");
   int ndev = 0;
   cudaError_t e = cudaGetDeviceCount(&ndev);
   if (e != cudaSuccess || ndev == 0) return fail(nullptr, TS_ERR_CUDA, "ts_create: no CUDA device");
@@ -206,6 +207,8 @@ ts_status ts_set_launch_config(ts_ctx *c, const ts_config *k) {
     return fail(c, TS_ERR_INVALID_ARG, "ts_set_launch_config: occupancy must be 0, 5 or 8");
   c->cfg.trace_budget = k->trace_budget > 0 ? k->trace_budget : 32;
   c->cfg.occupancy = k->occupancy;
+  if (k->queue_capacity < 0) return fail(c, TS_ERR_INVALID_ARG, "ts_set_launch_config: negative queue_capacity");
+  c->cfg.queue_capacity = k->queue_capacity;
   c->dc.speculative = k->traversal == TS_TRAVERSAL_SPECULATIVE ? 1 : 0;
   return TS_OK;
 }
@@ -499,7 +502,7 @@ ts_status ts_render_pass(ts_ctx *c, uint32_t pass_idx, int32_t band, void *strea
     if (per_sm <= 0) per_sm = std::max(1, 2048 / bs);
     const int grid = c->num_sms * per_sm;
     TS_CUDA(c, ts::launch_wave_pass(c->ds, c->dc, pass_idx, band, film_of(c), c->wave, c->d_err, grid, bs,
-                                    c->cfg.sort_keys, st, c->cfg.trace_budget),
+                                    c->cfg.sort_keys, st, c->cfg.trace_budget, c->cfg.queue_capacity),
             "render pass");
   }
   return TS_OK;
@@ -934,7 +937,8 @@ ts_status ts_batch_check(ts_batch *b, uint32_t *bits) {
 
 // wavefront buffers are created on first use (one slot per pixel)
 static ts_status ensure_wave(ts_ctx *c) {
-  const int n = c->cfg.width * c->cfg.height;
+  const int npix = c->cfg.width * c->cfg.height;
+  const int n = c->cfg.queue_capacity > 0 && c->cfg.queue_capacity < npix ? c->cfg.queue_capacity : npix;
   if (c->wave.capacity >= n) return TS_OK;
   free_list(c->wave_allocs);
   c->wave = ts::WaveBuffers{};

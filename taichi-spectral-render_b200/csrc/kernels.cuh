@@ -57,9 +57,10 @@ struct WaveBuffers {
 };
 constexpr int kMaxKeys = 256;
 
+// capacity: paths per chunk of the frame (0 = the whole frame); w holds at least that many slots
 cudaError_t launch_wave_pass(const DevScene &s, const DevConfig &c, uint32_t pass, int band, Film f,
                              const WaveBuffers &w, uint32_t *err, int grid, int block, int sort_keys,
-                             cudaStream_t st, int trace_budget);
+                             cudaStream_t st, int trace_budget, int capacity = 0);
 
 // ---- path-replay adjoint (adjoint.cu) -----------------------------------------
 constexpr int kAdjSharedMax = 4096;  // material-table gradients kept in shared memory (FP64, 32 KB)

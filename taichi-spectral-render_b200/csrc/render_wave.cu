@@ -57,19 +57,20 @@ __device__ __forceinline__ void deposit(const Film &f, int pixel, int band, floa
   if (v != 0.f) f.block[(size_t)band * f.W * f.H + pixel] += (double)v;
 }
 
-__global__ void k_generate(DevScene s, DevConfig c, uint32_t pass, int band, WaveBuffers w) {
-  const int npix = c.W * c.H;
-  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
+// camera rays of pixels [p0, p0 + n): path slot q <-> pixel p0 + q (pixel ids key the random streams)
+__global__ void k_generate(DevScene s, DevConfig c, uint32_t pass, int band, WaveBuffers w, int p0, int n) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    const int pix = p0 + q;
     Rng rng;
-    rng.init(c.seed, pass, (uint32_t)p, c.scene_id);
+    rng.init(c.seed, pass, (uint32_t)pix, c.scene_id);
     PathState ps;
-    camera_ray(s, c, p % c.W, p / c.W, rng, ps, band);
-    w.pos_thr[p] = make_float4(ps.pos.x, ps.pos.y, ps.pos.z, ps.thr);
-    w.dir_spdf[p] = make_float4(ps.dir.x, ps.dir.y, ps.dir.z, ps.spdf);
-    w.meta[p] = make_int4(p, band | (band << 8), 0, (int)rng.n);
-    w.queue[0][p] = p;
+    camera_ray(s, c, pix % c.W, pix / c.W, rng, ps, band);
+    w.pos_thr[q] = make_float4(ps.pos.x, ps.pos.y, ps.pos.z, ps.thr);
+    w.dir_spdf[q] = make_float4(ps.dir.x, ps.dir.y, ps.dir.z, ps.spdf);
+    w.meta[q] = make_int4(pix, band | (band << 8), 0, (int)rng.n);
+    w.queue[0][q] = q;
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) w.counts[kCntExt + 0] = npix;
+  if (blockIdx.x == 0 && threadIdx.x == 0) w.counts[kCntExt + 0] = n;
 }
 
 // trace(k): shadow chains of shade(k-1), then extension hits of Qk.
@@ -338,15 +339,32 @@ __global__ void __launch_bounds__(kMaxBlock) k_shade(DevScene s, DevConfig c, ui
 
 }  // namespace
 
+cudaError_t launch_wave_chunk(const DevScene &s, const DevConfig &c, uint32_t pass, int band, Film f,
+                              const WaveBuffers &w, uint32_t *err, int grid, int block, int sort_keys,
+                              cudaStream_t st, int trace_budget, int p0, int n);
+
 cudaError_t launch_wave_pass(const DevScene &s, const DevConfig &c, uint32_t pass, int band, Film f,
                              const WaveBuffers &w, uint32_t *err, int grid, int block, int sort_keys,
-                             cudaStream_t st, int trace_budget) {
+                             cudaStream_t st, int trace_budget, int capacity) {
+  // the frame in chunks of at most `capacity` paths (their queues stay in L2)
+  const int npix = c.W * c.H;
+  const int chunk = capacity > 0 && capacity < npix ? capacity : npix;
+  for (int p0 = 0; p0 < npix; p0 += chunk) {
+    const cudaError_t e = launch_wave_chunk(s, c, pass, band, f, w, err, grid, block, sort_keys, st, trace_budget, p0,
+                                            npix - p0 < chunk ? npix - p0 : chunk);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t launch_wave_chunk(const DevScene &s, const DevConfig &c, uint32_t pass, int band, Film f,
+                              const WaveBuffers &w, uint32_t *err, int grid, int block, int sort_keys,
+                              cudaStream_t st, int trace_budget, int p0, int n) {
   if (c.max_depth > kMaxDepth) return cudaErrorInvalidValue;
   cudaError_t e = cudaMemsetAsync(w.counts, 0, kCntTotal * sizeof(int), st);
   if (e != cudaSuccess) return e;
-  const int npix = c.W * c.H;
-  const int gen_grid = (npix + 255) / 256;
-  k_generate<<<gen_grid, 256, 0, st>>>(s, c, pass, band, w);
+  const int gen_grid = (n + 255) / 256;
+  k_generate<<<gen_grid, 256, 0, st>>>(s, c, pass, band, w, p0, n);
   // sort_keys bit 0: shading queue by material; bit 1: extension rays by
   // direction octant; bit 2: shadow queries by light triangle
   const int M = s.num_materials;

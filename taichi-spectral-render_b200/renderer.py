@@ -56,6 +56,7 @@ class RenderConfig:
     trace_budget: int = 0
     traversal: str = "default"      # two-child nodes: "default" (if-if loop) or "speculative" (while-while)
     occupancy: int = 0              # megakernel: 0 = 5 blocks/SM (96 registers), 8 = 8 blocks/SM (64 registers)
+    queue_capacity: int = 0         # wavefront: paths per chunk of the frame (0 = whole frame)
     device: int = 0
 
     @property
@@ -78,6 +79,7 @@ class RenderConfig:
         c.trace_budget = self.trace_budget
         c.traversal = {"default": 0, "speculative": 1}[self.traversal]
         c.occupancy = self.occupancy
+        c.queue_capacity = self.queue_capacity
         return c
 
 
@@ -142,11 +144,12 @@ class Renderer:
         _lib.check(status, self._ctx)
 
     def set_launch_config(self, kernel=None, traversal=None, block_size=None, blocks_per_sm=None, sort_keys=None,
-                          trace_budget=None, occupancy=None):
+                          trace_budget=None, occupancy=None, queue_capacity=None):
         """Change launch settings without re-uploading the scene (images do not depend on them)."""
         upd = {k: v for k, v in dict(kernel=kernel, traversal=traversal, block_size=block_size,
                                      blocks_per_sm=blocks_per_sm, sort_keys=sort_keys,
-                                     trace_budget=trace_budget, occupancy=occupancy).items() if v is not None}
+                                     trace_budget=trace_budget, occupancy=occupancy,
+                                     queue_capacity=queue_capacity).items() if v is not None}
         cfg = dataclasses.replace(self.config, **upd)
         self._check(self.lib.ts_set_launch_config(self._ctx, ctypes.byref(cfg.to_c())))
         self.config = cfg

@@ -27,8 +27,10 @@ def oracle_passes(comp, bvh, scene, cfg, passes, use_double=False):
     return out
 
 
-def gpu_passes(scene, cfg, ex, bvh, kernel, passes, sort_keys=0, node_width=0, traversal="default"):
-    c2 = sb.RenderConfig(**{**cfg.__dict__, "kernel": kernel, "sort_keys": sort_keys, "traversal": traversal})
+def gpu_passes(scene, cfg, ex, bvh, kernel, passes, sort_keys=0, node_width=0, traversal="default",
+               queue_capacity=0):
+    c2 = sb.RenderConfig(**{**cfg.__dict__, "kernel": kernel, "sort_keys": sort_keys, "traversal": traversal,
+                            "queue_capacity": queue_capacity})
     with sb.Renderer(scene, c2, eems=ex["eems"], cmf=ex["cmf"], bvh=bvh,
                      bvh_params={"width": node_width}) as r:
         for p in passes:
@@ -105,6 +107,28 @@ def test_wavefront_equals_megakernel():
         assert np.array_equal(b, e), w
     assert np.array_equal(b, gpu_passes(s, c, ex, bvh, "wavefront", passes, traversal="speculative"))
     assert np.array_equal(a, gpu_passes(s, c, ex, bvh, "mega", passes, traversal="speculative"))
+
+
+def test_wavefront_queue_capacity_changes_no_result():
+    """A pass rendered in chunks of the frame (ragged last chunk included) deposits
+    the same paths into the same cells as a whole-frame pass."""
+    s, c, ex, comp, bvh = setup(configs.volume_scene, width=64, height=64, medium_slices=30, medium_stacks=31,
+                                fluorescent_medium=True)
+    passes = range(10)
+    whole = gpu_passes(s, c, ex, bvh, "wavefront", passes)
+    for cap, sk in ((1000, 0), (777, 7), (4096, 1), (1 << 20, 0)):
+        assert np.array_equal(whole, gpu_passes(s, c, ex, bvh, "wavefront", passes, sort_keys=sk,
+                                                queue_capacity=cap)), cap
+    # a capacity set after the first pass (buffers already sized for the whole frame)
+    c2 = sb.RenderConfig(**{**c.__dict__, "kernel": "wavefront"})
+    with sb.Renderer(s, c2, eems=ex["eems"], cmf=ex["cmf"], bvh=bvh) as r:
+        for p in passes:
+            if p == 3:
+                r.set_launch_config(queue_capacity=513)
+            r.cast_rays(p % c.bands, pass_idx=p)
+        g = r.block_film.cpu().numpy().reshape(c.bands, -1).T.copy()
+        assert r.check_device() == 0
+    assert np.array_equal(whole, g)
 
 
 def test_statistical_parity_three_sigma():
@@ -233,6 +257,8 @@ def test_invalid_arguments_raise():
         nan["meshes"] = [m0]
         with pytest.raises(sb.SpectralError, match="non-finite"):
             r.setup_scene(nan, eems=ex["eems"], cmf=ex["cmf"])
+        with pytest.raises(sb.SpectralError, match="negative queue_capacity"):
+            r.set_launch_config(queue_capacity=-1)
         # the context stays usable after rejected uploads
         r.setup_scene(s, eems=ex["eems"], cmf=ex["cmf"], bvh=bvh)
         r.cast_rays(3)
