@@ -20,6 +20,7 @@ namespace {
 thread_local std::string g_last_error;
 
 constexpr int kMaxBands = 64;
+constexpr int kMaxQueueCapacity = 1 << 25;  // wavefront path slots (about 5.5 GB of path state)
 constexpr int kDefaultWidth = 2;  // BVH node width when the scene description leaves it at 0
 
 }  // namespace
@@ -45,6 +46,7 @@ struct ts_ctx {
   size_t adj_weight_cap = 0;      // entries
   ts::WaveBuffers wave{};
   std::vector<void *> wave_allocs;
+  ts::WaveLoopGraph *wave_loop = nullptr;  // captured regenerating wavefront loop
   size_t film_bytes = 0, scene_bytes = 0, wave_bytes = 0;
   float cam[9] = {0, 0, 3.5f, 0, 0, -1, 0, 1, 0};
   std::string err;
@@ -139,6 +141,8 @@ ts_status ts_create(const ts_config *cfg, ts_ctx **out) {
   if (k.occupancy != 0 && k.occupancy != 5 && k.occupancy != 8)
     return fail(nullptr, TS_ERR_INVALID_ARG, "ts_create: occupancy must be 0, 5 or 8");
   if (k.queue_capacity < 0) return fail(nullptr, TS_ERR_INVALID_ARG, "ts_create: negative queue_capacity");
+  if (k.queue_capacity > kMaxQueueCapacity)
+    return fail(nullptr, TS_ERR_INVALID_ARG, "ts_create: queue_capacity above 2^25 path slots");
   int ndev = 0;
   cudaError_t e = cudaGetDeviceCount(&ndev);
   if (e != cudaSuccess || ndev == 0) return fail(nullptr, TS_ERR_CUDA, "ts_create: no CUDA device");
@@ -208,6 +212,8 @@ ts_status ts_set_launch_config(ts_ctx *c, const ts_config *k) {
   c->cfg.trace_budget = k->trace_budget > 0 ? k->trace_budget : 32;
   c->cfg.occupancy = k->occupancy;
   if (k->queue_capacity < 0) return fail(c, TS_ERR_INVALID_ARG, "ts_set_launch_config: negative queue_capacity");
+  if (k->queue_capacity > kMaxQueueCapacity)
+    return fail(c, TS_ERR_INVALID_ARG, "ts_set_launch_config: queue_capacity above 2^25 path slots");
   c->cfg.queue_capacity = k->queue_capacity;
   c->dc.speculative = k->traversal == TS_TRAVERSAL_SPECULATIVE ? 1 : 0;
   return TS_OK;
@@ -217,6 +223,7 @@ ts_status ts_destroy(ts_ctx *c) {
   if (!c) return TS_OK;
   cudaSetDevice(c->cfg.device);
   free_list(c->scene_allocs);
+  ts::free_wave_loop(c->wave_loop);
   free_list(c->wave_allocs);
   for (double *p : c->d_film) cudaFree(p);
   cudaFree(c->d_counter);
@@ -481,6 +488,22 @@ ts_status ts_set_camera(ts_ctx *c, const float o[3], const float l[3], const flo
 
 static ts_status ensure_wave(ts_ctx *c);
 
+// wavefront passes through the regenerating loop: queue_capacity path slots
+// (one per pixel when 0)
+static ts_status render_wave_loop(ts_ctx *c, uint32_t pass0, int npass, int band0, cudaStream_t st, const char *what) {
+  const int64_t npix = (int64_t)c->cfg.width * c->cfg.height;
+  const int cap = c->cfg.queue_capacity > 0 ? c->cfg.queue_capacity : (int)npix;
+  if (npix * npass + cap > INT32_MAX)
+    return fail(c, TS_ERR_CAPACITY, std::string(what) + ": work items plus path slots exceed 2^31");
+  const int bs = c->cfg.block_size;
+  int per_sm = c->cfg.blocks_per_sm;
+  if (per_sm <= 0) per_sm = std::max(1, 2048 / bs);
+  TS_CUDA(c, ts::launch_wave_loop(c->ds, c->dc, pass0, band0, npass, film_of(c), c->wave, c->d_err,
+                                  c->num_sms * per_sm, bs, st, c->cfg.trace_budget, cap, &c->wave_loop),
+          what);
+  return TS_OK;
+}
+
 ts_status ts_render_pass(ts_ctx *c, uint32_t pass_idx, int32_t band, void *stream) {
   if (!c) return fail(nullptr, TS_ERR_INVALID_ARG, "ts_render_pass: null context");
   if (!c->has_scene) return fail(c, TS_ERR_NO_SCENE, "ts_render_pass: no scene uploaded");
@@ -501,6 +524,8 @@ ts_status ts_render_pass(ts_ctx *c, uint32_t pass_idx, int32_t band, void *strea
     int per_sm = c->cfg.blocks_per_sm;
     if (per_sm <= 0) per_sm = std::max(1, 2048 / bs);
     const int grid = c->num_sms * per_sm;
+    if (c->cfg.queue_capacity > 0 && c->cfg.sort_keys == 0)
+      return render_wave_loop(c, pass_idx, 1, band, st, "render pass");
     TS_CUDA(c, ts::launch_wave_pass(c->ds, c->dc, pass_idx, band, film_of(c), c->wave, c->d_err, grid, bs,
                                     c->cfg.sort_keys, st, c->cfg.trace_budget, c->cfg.queue_capacity),
             "render pass");
@@ -517,6 +542,12 @@ ts_status ts_render_passes(ts_ctx *c, uint32_t first_pass, int32_t num_passes, i
     return fail(c, TS_ERR_INVALID_ARG, "ts_render_passes: num_passes must be 1..bands (one film plane per pass)");
   if ((int64_t)num_passes * c->cfg.width * c->cfg.height > INT32_MAX)
     return fail(c, TS_ERR_CAPACITY, "ts_render_passes: more than 2^31 paths in one launch");
+  if (c->cfg.kernel != TS_KERNEL_MEGA && c->cfg.sort_keys == 0) {
+    cudaSetDevice(c->cfg.device);
+    const ts_status s = ensure_wave(c);
+    if (s != TS_OK) return s;
+    return render_wave_loop(c, first_pass, num_passes, first_band, as_stream(stream), "ts_render_passes");
+  }
   if (c->cfg.kernel != TS_KERNEL_MEGA) {
     for (int i = 0; i < num_passes; ++i) {
       const ts_status st = ts_render_pass(c, first_pass + (uint32_t)i, (first_band + i) % c->cfg.bands, stream);
@@ -938,7 +969,7 @@ ts_status ts_batch_check(ts_batch *b, uint32_t *bits) {
 // wavefront buffers are created on first use (one slot per pixel)
 static ts_status ensure_wave(ts_ctx *c) {
   const int npix = c->cfg.width * c->cfg.height;
-  const int n = c->cfg.queue_capacity > 0 && c->cfg.queue_capacity < npix ? c->cfg.queue_capacity : npix;
+  const int n = c->cfg.queue_capacity > 0 ? c->cfg.queue_capacity : npix;
   if (c->wave.capacity >= n) return TS_OK;
   free_list(c->wave_allocs);
   c->wave = ts::WaveBuffers{};
@@ -968,6 +999,8 @@ static ts_status ensure_wave(ts_ctx *c) {
   TS_CUDA(c, grab((void **)&w.shadow_order, N * sizeof(int)), "wavefront buffers");
   TS_CUDA(c, grab((void **)&w.counts, 8192 * sizeof(int)), "wavefront buffers");
   TS_CUDA(c, grab((void **)&w.key_hist, 2 * ts::kMaxKeys * sizeof(int)), "wavefront buffers");
+  TS_CUDA(c, grab((void **)&w.tag, N * sizeof(int)), "wavefront buffers");
+  TS_CUDA(c, grab((void **)&w.loop, sizeof(ts::WaveLoop)), "wavefront buffers");
   w.capacity = n;
   return TS_OK;
 }

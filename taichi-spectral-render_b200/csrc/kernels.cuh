@@ -36,6 +36,18 @@ cudaError_t launch_render_normals(const DevScene &s, const DevConfig &c, float *
                                   cudaStream_t st);
 
 // ---- wavefront renderer -------------------------------------------------------
+// state of the regenerating wavefront loop (render_wave.cu), device memory
+struct WaveLoop {
+  int ext[2];     // extension queue lengths: queue[a] is traced at the iterations of parity a
+  int sh[2];      // shadow queries appended by the shade of parity a
+  int fetch[2];   // trace / shade work counters of the current iteration
+  int next_item;  // next work item (pass offset * npix + pixel) to start
+  int total;      // work items of the launch
+  int iter, limit;
+  uint32_t pass0;
+  int band0, shared, pad_;
+};
+
 struct WaveBuffers {
   // path state, one slot per pixel
   float4 *pos_thr;    // pos.xyz, throughput
@@ -53,6 +65,8 @@ struct WaveBuffers {
   int *shadow_order;  // shadow query indices ordered by light triangle
   int *counts;        // [2*max_depth + 8]: ext counts per depth, shadow counts per depth, scratch
   int *key_hist;      // material-key histogram / offsets [kMaxKeys * 2]
+  int *tag;           // regenerating loop: path depth | pass offset << 16, per slot
+  WaveLoop *loop;     // regenerating loop state
   int capacity;
 };
 constexpr int kMaxKeys = 256;
@@ -61,6 +75,15 @@ constexpr int kMaxKeys = 256;
 cudaError_t launch_wave_pass(const DevScene &s, const DevConfig &c, uint32_t pass, int band, Film f,
                              const WaveBuffers &w, uint32_t *err, int grid, int block, int sort_keys,
                              cudaStream_t st, int trace_budget, int capacity = 0);
+
+// npass passes from pass0 / band0 (band wrapping mod B) over `capacity` path
+// slots (<= w.capacity) with path regeneration, as a CUDA-graph while-loop.
+// *graph caches the captured loop (rebuilt when a captured argument changes).
+struct WaveLoopGraph;
+cudaError_t launch_wave_loop(const DevScene &s, const DevConfig &c, uint32_t pass0, int band0, int npass, Film f,
+                             const WaveBuffers &w, uint32_t *err, int grid, int block, cudaStream_t st,
+                             int trace_budget, int capacity, WaveLoopGraph **graph);
+void free_wave_loop(WaveLoopGraph *graph);
 
 // ---- path-replay adjoint (adjoint.cu) -----------------------------------------
 constexpr int kAdjSharedMax = 4096;  // material-table gradients kept in shared memory (FP64, 32 KB)

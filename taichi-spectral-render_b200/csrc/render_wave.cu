@@ -17,7 +17,9 @@
 // atomics.  With sort_keys set, the shading queue is reordered by the hit
 // material (a counting sort on the device) so that warps shade one material
 // at a time.
+#include <cstring>
 #include <mutex>
+#include <vector>
 
 #include "estimator.cuh"
 #include "kernels.cuh"
@@ -53,21 +55,31 @@ __device__ __forceinline__ int warp_append(int *ctr, bool want) {
   return want ? base + __popc(m & ((1u << lane) - 1u)) : -1;
 }
 
-__device__ __forceinline__ void deposit(const Film &f, int pixel, int band, float v) {
-  if (v != 0.f) f.block[(size_t)band * f.W * f.H + pixel] += (double)v;
+// shared: several passes in flight may deposit into one cell (fluorescence
+// moves a deposit into another pass's band), so the add is atomic
+__device__ __forceinline__ void deposit(const Film &f, int pixel, int band, float v, bool shared = false) {
+  if (v == 0.f) return;
+  double *cell = f.block + (size_t)band * f.W * f.H + pixel;
+  if (shared) atomicAdd(cell, (double)v);
+  else *cell += (double)v;
 }
 
-// camera rays of pixels [p0, p0 + n): path slot q <-> pixel p0 + q (pixel ids key the random streams)
+// the camera ray of one pixel into path slot `slot` (the pixel id keys the random stream)
+__device__ __forceinline__ void start_path(const DevScene &s, const DevConfig &c, uint32_t pass, int band, int pix,
+                                           const WaveBuffers &w, int slot) {
+  Rng rng;
+  rng.init(c.seed, pass, (uint32_t)pix, c.scene_id);
+  PathState ps;
+  camera_ray(s, c, pix % c.W, pix / c.W, rng, ps, band);
+  w.pos_thr[slot] = make_float4(ps.pos.x, ps.pos.y, ps.pos.z, ps.thr);
+  w.dir_spdf[slot] = make_float4(ps.dir.x, ps.dir.y, ps.dir.z, ps.spdf);
+  w.meta[slot] = make_int4(pix, band | (band << 8), 0, (int)rng.n);
+}
+
+// camera rays of pixels [p0, p0 + n): path slot q <-> pixel p0 + q
 __global__ void k_generate(DevScene s, DevConfig c, uint32_t pass, int band, WaveBuffers w, int p0, int n) {
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-    const int pix = p0 + q;
-    Rng rng;
-    rng.init(c.seed, pass, (uint32_t)pix, c.scene_id);
-    PathState ps;
-    camera_ray(s, c, pix % c.W, pix / c.W, rng, ps, band);
-    w.pos_thr[q] = make_float4(ps.pos.x, ps.pos.y, ps.pos.z, ps.thr);
-    w.dir_spdf[q] = make_float4(ps.dir.x, ps.dir.y, ps.dir.z, ps.spdf);
-    w.meta[q] = make_int4(pix, band | (band << 8), 0, (int)rng.n);
+    start_path(s, c, pass, band, p0 + q, w, q);
     w.queue[0][q] = q;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) w.counts[kCntExt + 0] = n;
@@ -77,16 +89,30 @@ __global__ void k_generate(DevScene s, DevConfig c, uint32_t pass, int band, Wav
 // Persistent lanes with per-lane refill: each lane traverses its current ray
 // for at most `budget` steps; lanes whose ray has finished then take new work
 // items (one atomic per warp), so a warp does not idle behind its longest ray.
-template <int W>
+// kLoop: one iteration of the regenerating loop (queue lengths from *L).
+template <int W, bool kLoop = false>
 __global__ void __launch_bounds__(kMaxBlock, 4) k_trace(DevScene s, DevConfig c, int depth, Film f, WaveBuffers w,
                                                      uint32_t *__restrict__ err, int budget, int ext_sorted,
-                                                     int shadow_sorted) {
+                                                     int shadow_sorted, WaveLoop *L) {
   uint32_t eb = 0;
-  const int nsh = depth > 0 ? w.counts[kCntSh + depth - 1] : 0;
-  const int next = depth < c.max_depth ? w.counts[kCntExt + depth] : 0;
-  const int *q = ext_sorted ? w.trace_order : w.queue[depth & 1];
+  int nsh, next, *fetch;
+  const int *q;
+  bool shared = false;
+  if (kLoop) {
+    const int a = L->iter & 1;
+    nsh = L->sh[a ^ 1];
+    next = L->ext[a];
+    q = w.queue[a];
+    fetch = L->fetch + 0;
+    shared = L->shared != 0;
+    ext_sorted = shadow_sorted = 0;
+  } else {
+    nsh = depth > 0 ? w.counts[kCntSh + depth - 1] : 0;
+    next = depth < c.max_depth ? w.counts[kCntExt + depth] : 0;
+    q = ext_sorted ? w.trace_order : w.queue[depth & 1];
+    fetch = w.counts + kCntFetchT + depth;
+  }
   const int total = nsh + next;
-  int *fetch = w.counts + kCntFetchT + depth;
   const int lane = threadIdx.x & 31;
   int item = -1, pid = 0, pixel = 0, band = 0, dep_band = 0;
   bool exhausted = false;
@@ -138,7 +164,7 @@ __global__ void __launch_bounds__(kMaxBlock, 4) k_trace(DevScene s, DevConfig c,
     if (item >= 0 && trav_advance<W>(s, t, stack, c.eps, budget, eb)) {
       if (item < nsh) {
         if (shadow_segment(s, c, sq, t.h, band, ss)) {
-          if (ss.total > 1e-6f) deposit(f, pixel, dep_band, sq.contrib * ss.total);
+          if (ss.total > 1e-6f) deposit(f, pixel, dep_band, sq.contrib * ss.total, shared);
           item = -1;
         } else {
           trav_begin(s, t, ss.pos, sq.dir, shadow_bound(s, c, sq, ss, band));
@@ -152,16 +178,18 @@ __global__ void __launch_bounds__(kMaxBlock, 4) k_trace(DevScene s, DevConfig c,
   if (eb) atomicOr(err, eb);
 }
 
+template <bool kLoop = false>
 void launch_trace(const DevScene &s, const DevConfig &c, int depth, Film f, const WaveBuffers &w, uint32_t *err,
-                  int grid, int block, cudaStream_t st, int budget, int ext_sorted = 0, int shadow_sorted = 0) {
+                  int grid, int block, cudaStream_t st, int budget, int ext_sorted = 0, int shadow_sorted = 0,
+                  WaveLoop *L = nullptr) {
   if (s.node_width == 8)
-    k_trace<8><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget, ext_sorted, shadow_sorted);
+    k_trace<8, kLoop><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget, ext_sorted, shadow_sorted, L);
   else if (s.node_width == 4)
-    k_trace<4><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget, ext_sorted, shadow_sorted);
+    k_trace<4, kLoop><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget, ext_sorted, shadow_sorted, L);
   else if (c.speculative)
-    k_trace<3><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget, ext_sorted, shadow_sorted);
+    k_trace<3, kLoop><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget, ext_sorted, shadow_sorted, L);
   else
-    k_trace<2><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget, ext_sorted, shadow_sorted);
+    k_trace<2, kLoop><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget, ext_sorted, shadow_sorted, L);
 }
 
 // ---- queue sorting ------------------------------------------------------
@@ -250,91 +278,220 @@ void launch_sort(const DevScene &s, int depth, const WaveBuffers &w, int kind, i
   k_sort_scatter<<<grid, 256, 0, st>>>(s, depth, w, kind, nkeys, out);
 }
 
+// one path of an extension queue: volume event, emitter hit, next-event setup
+// and surface or volume scatter.  cont: the path goes on (its state was
+// written back); nee: r.sq is its shadow query.  last: no further vertex.
+struct Shaded {
+  bool cont, nee;
+  int pix, dep_band;
+  ShadowQuery sq;
+};
+
+__device__ __forceinline__ void shade_path(const DevScene &s, const DevConfig &c, uint32_t pass, int band, bool last,
+                                           const Film &f, const WaveBuffers &w, int pid, bool shared, Shaded &r) {
+  const float4 pt = w.pos_thr[pid], ds = w.dir_spdf[pid];
+  const int4 m = w.meta[pid];
+  const float4 hh = w.hit[pid];
+  r.pix = m.x;
+  PathState p;
+  p.pos = xyz(pt);
+  p.thr = pt.w;
+  p.dir = xyz(ds);
+  p.spdf = ds.w;
+  p.active = m.y & 0xff;
+  p.active_px = (m.y >> 8) & 0xff;
+  p.plen = (m.y >> 16) & 0xffff;
+  p.vol = m.z;
+  Rng rng;
+  rng.init(c.seed, pass, (uint32_t)m.x, c.scene_id, (uint32_t)m.w);
+  Hit h;
+  h.t = hh.x;
+  h.u = hh.y;
+  h.v = hh.z;
+  h.slot = __float_as_int(hh.w);
+  const VolEvent ev = volume_event(s, c, p, h, rng);
+  if (ev.travel < 0.f) return;
+  p.pos = p.pos + p.dir * ev.travel;
+  p.thr *= ev.est;
+  bool done = false;
+  float indirect = 0.f;
+  if (ev.action == 1) {
+    const Mat sm = get_mat(s, c.B, ev.hit_mat, band);
+    if (sm.surf_emis) {
+      indirect = emitter_hit(s, c, p, ev, sm.emission);
+      done = true;
+    } else {
+      r.nee = nee_setup(s, c, p, band, ev.snormal, ev.hit_mat, rng, r.sq);
+    }
+  } else {
+    r.nee = nee_setup(s, c, p, band, ev.snormal, -1, rng, r.sq);
+  }
+  r.sq.band = p.active;
+  if (ev.action == 1 && !done) {
+    p.plen++;
+    const SurfEvent se = scatter_surface(s, c, p, ev, rng);
+    apply_surface(c, p, ev, se);
+  } else if (ev.action == 2) {
+    p.dir = ev.dir;
+    p.plen++;
+  } else if (ev.action == 3) {
+    p.dir = ev.dir;
+    p.active = ev.new_wl;
+    p.active_px = ev.new_wl;
+    p.plen++;
+  }
+  r.dep_band = p.active_px;
+  deposit(f, m.x, r.dep_band, indirect, shared);
+  r.cont = !done && !last && p.thr != 0.f;
+  if (r.cont) {
+    w.pos_thr[pid] = make_float4(p.pos.x, p.pos.y, p.pos.z, p.thr);
+    w.dir_spdf[pid] = make_float4(p.dir.x, p.dir.y, p.dir.z, p.spdf);
+    w.meta[pid] = make_int4(m.x, p.active | (p.active_px << 8) | (p.plen << 16), p.vol, (int)rng.n);
+  }
+}
+
+__device__ __forceinline__ void append_shadow(int *count, const WaveBuffers &w, const Shaded &r) {
+  const int sslot = warp_append(count, r.nee);
+  if (r.nee) {
+    w.sq_origin[sslot] = make_float4(r.sq.origin.x, r.sq.origin.y, r.sq.origin.z, r.sq.max_dist);
+    w.sq_dir[sslot] = make_float4(r.sq.dir.x, r.sq.dir.y, r.sq.dir.z, r.sq.contrib);
+    w.sq_meta[sslot] = make_int4(r.pix, r.sq.light_slot, r.sq.vol, r.sq.band | (r.dep_band << 8));
+  }
+}
+
 __global__ void __launch_bounds__(kMaxBlock) k_shade(DevScene s, DevConfig c, uint32_t pass, int band, int depth,
                                                Film f, WaveBuffers w, int use_sorted) {
   const int n = w.counts[kCntExt + depth];
   const int *q = use_sorted ? w.sorted : w.queue[depth & 1];
   int *qn = w.queue[(depth + 1) & 1];
   int *fetch = w.counts + kCntFetchS + depth;
+  const bool last = depth + 1 >= c.max_depth;
   for (;;) {
     const int base = warp_fetch(fetch);
     if (base >= n) break;
     const int i = base + (threadIdx.x & 31);
-    bool cont = false, nee = false;
-    int pid = -1, pix = -1, dep_band = 0;
-    ShadowQuery sq;
-    PathState p;
-    Rng rng;
+    Shaded r;
+    r.cont = r.nee = false;
+    r.pix = -1;
+    r.dep_band = 0;
+    int pid = -1;
     if (i < n) {
       pid = q[i];
-      const float4 pt = w.pos_thr[pid], ds = w.dir_spdf[pid];
-      const int4 m = w.meta[pid];
-      const float4 hh = w.hit[pid];
-      pix = m.x;
-      p.pos = xyz(pt);
-      p.thr = pt.w;
-      p.dir = xyz(ds);
-      p.spdf = ds.w;
-      p.active = m.y & 0xff;
-      p.active_px = (m.y >> 8) & 0xff;
-      p.plen = (m.y >> 16) & 0xffff;
-      p.vol = m.z;
-      rng.init(c.seed, pass, (uint32_t)m.x, c.scene_id, (uint32_t)m.w);
-      Hit h;
-      h.t = hh.x;
-      h.u = hh.y;
-      h.v = hh.z;
-      h.slot = __float_as_int(hh.w);
-      const VolEvent ev = volume_event(s, c, p, h, rng);
-      if (ev.travel >= 0.f) {
-        p.pos = p.pos + p.dir * ev.travel;
-        p.thr *= ev.est;
-        bool done = false;
-        float indirect = 0.f;
-        if (ev.action == 1) {
-          const Mat sm = get_mat(s, c.B, ev.hit_mat, band);
-          if (sm.surf_emis) {
-            indirect = emitter_hit(s, c, p, ev, sm.emission);
-            done = true;
-          } else {
-            nee = nee_setup(s, c, p, band, ev.snormal, ev.hit_mat, rng, sq);
-          }
-        } else {
-          nee = nee_setup(s, c, p, band, ev.snormal, -1, rng, sq);
-        }
-        sq.band = p.active;
-        if (ev.action == 1 && !done) {
-          p.plen++;
-          const SurfEvent se = scatter_surface(s, c, p, ev, rng);
-          apply_surface(c, p, ev, se);
-        } else if (ev.action == 2) {
-          p.dir = ev.dir;
-          p.plen++;
-        } else if (ev.action == 3) {
-          p.dir = ev.dir;
-          p.active = ev.new_wl;
-          p.active_px = ev.new_wl;
-          p.plen++;
-        }
-        dep_band = p.active_px;
-        deposit(f, m.x, dep_band, indirect);
-        cont = !done && depth + 1 < c.max_depth && p.thr != 0.f;
-        if (cont) {
-          w.pos_thr[pid] = make_float4(p.pos.x, p.pos.y, p.pos.z, p.thr);
-          w.dir_spdf[pid] = make_float4(p.dir.x, p.dir.y, p.dir.z, p.spdf);
-          w.meta[pid] = make_int4(m.x, p.active | (p.active_px << 8) | (p.plen << 16), p.vol, (int)rng.n);
-        }
+      shade_path(s, c, pass, band, last, f, w, pid, false, r);
+    }
+    append_shadow(w.counts + kCntSh + depth, w, r);
+    const int qslot = warp_append(w.counts + kCntExt + depth + 1, r.cont);
+    if (r.cont) qn[qslot] = pid;
+  }
+}
+
+// ---- the regenerating loop ----------------------------------------------
+// A launch of npass passes (a wavelength bundle, or one pass) as work items
+// idx = pass offset * npix + pixel over `capacity` path slots.  One iteration
+// is trace (the shadow queries of the last shade and the extension rays of
+// the queue) then shade, in which every slot whose path has ended starts the
+// next work item at once, so the queue stays full until the items run out
+// and the long-path tail is paid once per launch, not once per pass.  The
+// iterations run as the body of a CUDA-graph while-loop whose condition the
+// control kernel sets: no host round trip decides when a launch is done.
+//
+// Slot tag: path depth | pass offset << 16.  Each cell of a pass's band plane
+// has one path per pass, so deposits are plain adds unless passes in flight
+// share cells (several passes with fluorescence moving deposits across bands).
+
+// paths [0, n0) of the launch into slots [0, n0), and the loop state
+__global__ void k_loop_init(DevScene s, DevConfig c, WaveBuffers w, WaveLoop *L, uint32_t pass0, int band0,
+                            int npass, int n0, int limit, int shared) {
+  const int npix = c.W * c.H;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n0; q += gridDim.x * blockDim.x) {
+    const int po = q / npix;
+    int band = band0 + po;
+    if (band >= c.B) band -= c.B;
+    start_path(s, c, pass0 + (uint32_t)po, band, q - po * npix, w, q);
+    w.tag[q] = po << 16;
+    w.queue[0][q] = q;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    L->ext[0] = n0;
+    L->ext[1] = 0;
+    L->sh[0] = L->sh[1] = 0;
+    L->fetch[0] = L->fetch[1] = 0;
+    L->next_item = n0;
+    L->total = npass * npix;
+    L->iter = 0;
+    L->limit = limit;
+    L->pass0 = pass0;
+    L->band0 = band0;
+    L->shared = shared;
+  }
+}
+
+__global__ void __launch_bounds__(kMaxBlock) k_shade_loop(DevScene s, DevConfig c, Film f, WaveBuffers w, WaveLoop *L) {
+  const int a = L->iter & 1;
+  const int n = L->ext[a];
+  const int *q = w.queue[a];
+  int *qn = w.queue[a ^ 1];
+  const uint32_t pass0 = L->pass0;
+  const int band0 = L->band0, total = L->total;
+  const bool shared = L->shared != 0;
+  // items left to start, read once: the item counter then overshoots the
+  // total by at most one claim per slot
+  const bool more = L->next_item < total;
+  const int npix = c.W * c.H;
+  for (;;) {
+    const int base = warp_fetch(L->fetch + 1);
+    if (base >= n) break;
+    const int i = base + (threadIdx.x & 31);
+    Shaded r;
+    r.cont = r.nee = false;
+    r.pix = -1;
+    r.dep_band = 0;
+    int pid = -1;
+    if (i < n) {
+      pid = q[i];
+      const int tag = w.tag[pid];
+      const int po = tag >> 16;
+      int band = band0 + po;
+      if (band >= c.B) band -= c.B;
+      shade_path(s, c, pass0 + (uint32_t)po, band, (tag & 0xffff) + 1 >= c.max_depth, f, w, pid, shared, r);
+      if (r.cont) w.tag[pid] = tag + 1;
+    }
+    append_shadow(L->sh + a, w, r);
+    // the slots of ended paths start the next work items
+    bool fresh = false;
+    if (more) {
+      const int item = warp_append(&L->next_item, pid >= 0 && !r.cont);
+      if (item >= 0 && item < total) {
+        const int po = item / npix;
+        int band = band0 + po;
+        if (band >= c.B) band -= c.B;
+        start_path(s, c, pass0 + (uint32_t)po, band, item - po * npix, w, pid);
+        w.tag[pid] = po << 16;
+        fresh = true;
       }
     }
-    const int sslot = warp_append(w.counts + kCntSh + depth, nee);
-    if (nee) {
-      w.sq_origin[sslot] = make_float4(sq.origin.x, sq.origin.y, sq.origin.z, sq.max_dist);
-      w.sq_dir[sslot] = make_float4(sq.dir.x, sq.dir.y, sq.dir.z, sq.contrib);
-      w.sq_meta[sslot] = make_int4(pix, sq.light_slot, sq.vol, sq.band | (dep_band << 8));
-    }
-    const int qslot = warp_append(w.counts + kCntExt + depth + 1, cont);
-    if (cont) qn[qslot] = pid;
+    const int qslot = warp_append(L->ext + (a ^ 1), r.cont || fresh);
+    if (r.cont || fresh) qn[qslot] = pid;
   }
+}
+
+// end of an iteration: go on while rays or shadow queries are queued, reset
+// the counters the next iteration appends to, and stop (with an error bit) at
+// the iteration bound, which no launch reaches unless the queues are corrupt
+__global__ void k_loop_control(WaveLoop *L, cudaGraphConditionalHandle h, uint32_t *err) {
+  if (threadIdx.x != 0) return;
+  const int a = L->iter & 1;
+  bool go = L->ext[a ^ 1] > 0 || L->sh[a] > 0;
+  L->ext[a] = 0;
+  L->sh[a ^ 1] = 0;
+  L->fetch[0] = L->fetch[1] = 0;
+  const int it = L->iter + 1;
+  L->iter = it;
+  if (go && it >= L->limit) {
+    atomicOr(err, kErrIterationCap);
+    go = false;
+  }
+  cudaGraphSetConditional(h, go ? 1u : 0u);
 }
 
 }  // namespace
@@ -390,6 +547,105 @@ cudaError_t launch_wave_chunk(const DevScene &s, const DevConfig &c, uint32_t pa
     launch_trace(s, c, c.max_depth, f, w, err, grid, block, st, trace_budget, 0, sh_sorted);
   }
   return cudaGetLastError();
+}
+
+struct WaveLoopGraph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t capture = nullptr;
+  std::vector<unsigned char> key;  // the captured kernel arguments
+};
+
+void free_wave_loop(WaveLoopGraph *g) {
+  if (!g) return;
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  if (g->capture) cudaStreamDestroy(g->capture);
+  delete g;
+}
+
+namespace {
+
+cudaError_t build_wave_loop(WaveLoopGraph &G, const DevScene &s, const DevConfig &c, Film f, const WaveBuffers &w,
+                            uint32_t *err, int grid, int block, int budget) {
+  if (G.exec) cudaGraphExecDestroy(G.exec);
+  if (G.graph) cudaGraphDestroy(G.graph);
+  G.exec = nullptr;
+  G.graph = nullptr;
+  cudaError_t e;
+  if (!G.capture && (e = cudaStreamCreateWithFlags(&G.capture, cudaStreamNonBlocking)) != cudaSuccess) return e;
+  if ((e = cudaGraphCreate(&G.graph, 0)) != cudaSuccess) return e;
+  cudaGraphConditionalHandle h;
+  if ((e = cudaGraphConditionalHandleCreate(&h, G.graph, 1, cudaGraphCondAssignDefault)) != cudaSuccess) return e;
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  if ((e = cudaGraphAddNode(&node, G.graph, nullptr, 0, &cp)) != cudaSuccess) return e;
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  if ((e = cudaStreamBeginCaptureToGraph(G.capture, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)) !=
+      cudaSuccess)
+    return e;
+  launch_trace<true>(s, c, 0, f, w, err, grid, block, G.capture, budget, 0, 0, w.loop);
+  k_shade_loop<<<grid, block, 0, G.capture>>>(s, c, f, w, w.loop);
+  k_loop_control<<<1, 32, 0, G.capture>>>(w.loop, h, err);
+  const cudaError_t le = cudaGetLastError();
+  cudaGraph_t captured = nullptr;
+  e = cudaStreamEndCapture(G.capture, &captured);
+  if (le != cudaSuccess) return le;
+  if (e != cudaSuccess) return e;
+  return cudaGraphInstantiate(&G.exec, G.graph, 0);
+}
+
+}  // namespace
+
+cudaError_t launch_wave_loop(const DevScene &s, const DevConfig &c, uint32_t pass0, int band0, int npass, Film f,
+                             const WaveBuffers &w, uint32_t *err, int grid, int block, cudaStream_t st,
+                             int trace_budget, int capacity, WaveLoopGraph **graph) {
+  const int64_t npix = (int64_t)c.W * c.H;
+  const int64_t total = npix * npass;
+  if (c.max_depth > kMaxDepth || npass < 1 || npass > 32767 || capacity < 1 || capacity > w.capacity ||
+      !w.tag || !w.loop || total + capacity > INT32_MAX)
+    return cudaErrorInvalidValue;
+  const int n0 = (int)(total < capacity ? total : capacity);
+  // every slot starts a new item at least once per max_depth iterations while
+  // items are left, and a path lives at most max_depth iterations
+  const int64_t bound = ((total + n0 - 1) / n0 + 2) * (int64_t)(c.max_depth + 1) + 4;
+  const int limit = (int)(bound < INT32_MAX ? bound : INT32_MAX);
+  const int shared = npass > 1 && s.num_eems > 0 ? 1 : 0;
+  struct Key {
+    DevScene s;
+    DevConfig c;
+    Film f;
+    WaveBuffers w;
+    uint32_t *err;
+    int grid, block, budget;
+  } k;
+  memset(&k, 0, sizeof k);
+  memcpy(&k.s, &s, sizeof s);
+  memcpy(&k.c, &c, sizeof c);
+  memcpy(&k.f, &f, sizeof f);
+  memcpy(&k.w, &w, sizeof w);
+  k.err = err;
+  k.grid = grid;
+  k.block = block;
+  k.budget = trace_budget;
+  const unsigned char *kb = reinterpret_cast<const unsigned char *>(&k);
+  if (!*graph) *graph = new WaveLoopGraph;
+  WaveLoopGraph &G = **graph;
+  if (!G.exec || G.key.size() != sizeof k || memcmp(G.key.data(), kb, sizeof k) != 0) {
+    G.key.clear();
+    const cudaError_t e = build_wave_loop(G, s, c, f, w, err, grid, block, trace_budget);
+    if (e != cudaSuccess) return e;
+    G.key.assign(kb, kb + sizeof k);
+  }
+  const int init_grid = (int)((n0 + 255) / 256 < 4096 ? (n0 + 255) / 256 : 4096);
+  k_loop_init<<<init_grid, 256, 0, st>>>(s, c, w, w.loop, pass0, band0, npass, n0, limit, shared);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return cudaGraphLaunch(G.exec, st);
 }
 
 // ---------------------------------------------------------------------------

@@ -131,6 +131,54 @@ def test_wavefront_queue_capacity_changes_no_result():
     assert np.array_equal(whole, g)
 
 
+def gpu_bundles(scene, cfg, ex, bvh, kernel, bundles, queue_capacity=0, sort_keys=0):
+    """(first_pass, first_band, num_passes) launches into one film."""
+    c2 = sb.RenderConfig(**{**cfg.__dict__, "kernel": kernel, "queue_capacity": queue_capacity,
+                            "sort_keys": sort_keys})
+    with sb.Renderer(scene, c2, eems=ex["eems"], cmf=ex["cmf"], bvh=bvh) as r:
+        for p0, b0, n in bundles:
+            r.cast_rays_bundle(b0, n, pass_idx=p0)
+        g = r.block_film.cpu().numpy().reshape(cfg.bands, -1).T.copy()
+        assert r.check_device() == 0
+    return g
+
+
+def test_wavefront_regenerating_loop_single_pass():
+    """queue_capacity > 0: a pass over fewer (or more) path slots than pixels,
+    slots of ended paths starting the next pixels; the same paths and deposits
+    as the depth-synchronous pass."""
+    s, c, ex, comp, bvh = setup(configs.box_scene, width=48, height=48)
+    passes = range(25)
+    whole = gpu_passes(s, c, ex, bvh, "wavefront", passes)
+    for cap in (1, 97, 1000, 48 * 48, 10000):
+        assert np.array_equal(whole, gpu_passes(s, c, ex, bvh, "wavefront", passes, queue_capacity=cap)), cap
+
+
+def test_wavefront_regenerating_loop_bundles():
+    """A wavelength bundle through the wavefront loop: bit-identical to one pass
+    per launch where no fluorescence moves deposits between bands; with it, the
+    same deposits summed in another order."""
+    s, c, ex, comp, bvh = setup(configs.box_scene, width=48, height=48)
+    per_pass = gpu_passes(s, c, ex, bvh, "wavefront", range(50))
+    for cap in (0, 500, 3 * 48 * 48):
+        g = gpu_bundles(s, c, ex, bvh, "wavefront", [(0, 0, 25), (25, 0, 25)], queue_capacity=cap)
+        assert np.array_equal(per_pass, g), cap
+    # bundles that start mid-block and wrap the band index
+    per_pass = gpu_passes(s, c, ex, bvh, "wavefront", range(7, 27))
+    assert np.array_equal(per_pass, gpu_bundles(s, c, ex, bvh, "wavefront", [(7, 7, 11), (18, 18, 9)],
+                                                queue_capacity=300))
+    s, c, ex, comp, bvh = setup(configs.volume_scene, width=40, height=40, medium_slices=30, medium_stacks=31,
+                                fluorescent_medium=True, depth=16)
+    per_pass = gpu_passes(s, c, ex, bvh, "wavefront", range(25))
+    mega = gpu_bundles(s, c, ex, bvh, "mega", [(0, 0, 25)])
+    for cap in (0, 700, 10 * 1600):
+        g = gpu_bundles(s, c, ex, bvh, "wavefront", [(0, 0, 25)], queue_capacity=cap)
+        assert np.allclose(per_pass, g, rtol=1e-12, atol=1e-15), cap
+        assert np.allclose(mega, g, rtol=1e-12, atol=1e-15), cap
+    # sorted queues keep one launch per pass (depth-synchronous stages)
+    assert np.array_equal(per_pass, gpu_bundles(s, c, ex, bvh, "wavefront", [(0, 0, 25)], sort_keys=1))
+
+
 def test_statistical_parity_three_sigma():
     """Independent streams: per-cell means agree within 3 combined standard errors."""
     s, c, ex, comp, bvh = setup(configs.box_scene, width=16, height=16)
