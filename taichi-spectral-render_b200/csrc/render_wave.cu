@@ -609,6 +609,7 @@ cudaError_t launch_wave_loop(const DevScene &s, const DevConfig &c, uint32_t pas
   if (c.max_depth > kMaxDepth || npass < 1 || npass > 32767 || capacity < 1 || capacity > w.capacity ||
       !w.tag || !w.loop || total + capacity > INT32_MAX)
     return cudaErrorInvalidValue;
+  if (c.max_depth <= 0) return cudaSuccess;  // no vertex: nothing is deposited (as in the depth-synchronous pass)
   const int n0 = (int)(total < capacity ? total : capacity);
   // every slot starts a new item at least once per max_depth iterations while
   // items are left, and a path lives at most max_depth iterations
