@@ -47,6 +47,8 @@ def parse():
     p.add_argument("--launch", default="bundle", choices=["bundle", "pass"],
                    help="render the timed passes 25 per launch (wavelength bundles) or one per launch")
     p.add_argument("--budget", type=int, default=0, help="wavefront traversal steps between refills")
+    p.add_argument("--queue-capacity", type=int, default=0,
+                   help="wavefront path slots of the regenerating loop (--no-tune; 0 = one per pixel)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-extras", action="store_true", help="skip the time-to-RMSE and adjoint-cost legs")
     p.add_argument("--no-tune", action="store_true", help="use --kernel/--width/--traversal as given instead of "
@@ -205,7 +207,8 @@ def rmse_leg(name, target, seconds, bundles=True):
     from spectral_b200 import batch as sbatch
     from spectral_b200 import autotune
     scene, cfg, ex, desc = workload(name)
-    # megakernel launch settings from the autotuner (bundles need the megakernel)
+    # launch settings from the autotuner: for bundles the megakernel and the
+    # regenerating wavefront loop (queue capacities), per pass the megakernel
     cands = [c for c in autotune.default_candidates(quick=True) if c.kernel == "mega"]
     best, _ = autotune.tune(scene, cfg, eems=ex["eems"], cmf=ex["cmf"], candidates=cands, passes=50 if bundles else 6,
                             first_pass=1 << 26, bundles=bundles)
@@ -238,8 +241,9 @@ def rmse_leg(name, target, seconds, bundles=True):
     secs = time.perf_counter() - t0
     est = sbatch.relative_rmse_estimate(r, nb)
     out = {"workload": name, "target": target, "blocks": nb, "spp": nb * B, "seconds": secs,
-           "launch": {"width": best.width, "traversal": best.traversal, "block_size": best.block_size,
-                      "blocks_per_sm": best.blocks_per_sm, "occupancy": best.occupancy},
+           "launch": {"kernel": best.kernel, "width": best.width, "traversal": best.traversal,
+                      "block_size": best.block_size, "blocks_per_sm": best.blocks_per_sm,
+                      "occupancy": best.occupancy, "queue_capacity": best.queue_capacity},
            "estimated_rmse": float(est), "reached": bool(est <= target),
            "launches": "one per block (wavelength bundle)" if bundles else "one per pass"}
     if est > target:
@@ -471,11 +475,13 @@ def bench_ours(args):
     cfg.traversal = args.traversal
     cfg.trace_budget = args.budget
     cfg.occupancy = args.occupancy
+    cfg.queue_capacity = args.queue_capacity
     cfg.device = local
     tuned = None
     if not args.no_tune:
         # launch configuration chosen by the autotuner (megakernel candidates: BVH width,
-        # traversal loop, block shape); every candidate renders the same paths
+        # traversal loop, block shape, register budget; for bundles also the regenerating
+        # wavefront loop's queue capacity); every candidate renders the same paths
         from spectral_b200 import autotune
         t0 = time.time()
         bundles = args.launch == "bundle"
@@ -486,9 +492,9 @@ def bench_ours(args):
         tuned = {"seconds": time.time() - t0, "candidates": len(table),
                  "best": {"width": best.width, "traversal": best.traversal, "kernel": best.kernel,
                           "block_size": best.block_size, "blocks_per_sm": best.blocks_per_sm,
-                          "occupancy": best.occupancy},
+                          "occupancy": best.occupancy, "queue_capacity": best.queue_capacity},
                  "ms_per_pass": {f"w{c.width}/{c.traversal}/{c.kernel}/b{c.block_size}/s{c.blocks_per_sm}"
-                                 f"/o{c.occupancy}": round(ms, 4) for c, ms in table}}
+                                 f"/o{c.occupancy}/q{c.queue_capacity}": round(ms, 4) for c, ms in table}}
     comp = sb.compile_scene(scene, cfg.bands, eems=ex["eems"], cmf=ex["cmf"])
     bvh = sb._lib.build_bvh_host(comp.tris["v0"], comp.tris["v1"], comp.tris["v2"])
     r = sb.Renderer(scene, cfg, eems=ex["eems"], cmf=ex["cmf"], bvh=bvh, bvh_params={"width": args.width})
@@ -513,7 +519,9 @@ def bench_ours(args):
     sampler.start()
     time.sleep(0.3)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    use_bundles = args.launch == "bundle" and args.kernel == "mega"
+    # wavelength bundles: the megakernel, or the wavefront's regenerating loop (unsorted queues)
+    use_bundles = args.launch == "bundle" and (args.kernel == "mega" or cfg.sort_keys == 0)
+    wave_loop = args.kernel == "wavefront" and (use_bundles or cfg.queue_capacity > 0) and cfg.sort_keys == 0
     e0.record()
     k = 0
     while k < args.steps:  # exactly K passes; whole wavelength bundles when asked, single passes after
@@ -537,17 +545,28 @@ def bench_ours(args):
     value = world * args.steps * paths_per_step / (ms_max * 1e-3) / 1e6
     bits = r.check_device()
 
-    # ---- end to end through the public API with host buffers: camera in,
-    # resolved XYZ image out (pinned), every step
+    loop_iters = r.wave_loop_iterations() if wave_loop else 0  # of the last timed launch
+
+    # ---- end to end through the public API with host buffers, at the
+    # reference's cadence (main.py:1826-1837): per step the camera in, one
+    # block of B passes, the block folded into the running mean
+    # (average_and_reset_block) and the resolved XYZ image out (pinned)
     out = torch.empty((cfg.height, cfg.width, 3), dtype=torch.float32, pin_memory=True).numpy()
     cam = scene["camera"]
-    e2e_steps = max(10, args.steps // 3)
+    e2e_blocks = max(4, args.steps // B // 2)
+    r.clear_pixel_space()
     torch.cuda.synchronize()
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     f0.record()
-    for k in range(e2e_steps):
+    for k in range(e2e_blocks):
         r.update_camera(cam["origin"], cam["lookat"], cam["up"])
-        r.cast_rays(k % B, pass_idx=base_pass + 7 * (args.steps + 1) + k)
+        p0 = base_pass + 7 * (args.steps + 1) + k * B
+        if use_bundles:
+            r.cast_rays_bundle(0, B, pass_idx=p0)
+        else:
+            for b in range(B):
+                r.cast_rays(b, pass_idx=p0 + b)
+        r.average_and_reset_block(k + 1)
         r.resolve_xyz_host(out)
     f1.record()
     torch.cuda.synchronize()
@@ -555,24 +574,30 @@ def bench_ours(args):
     t2 = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(t2, op=dist.ReduceOp.MAX)
-    e2e_value = world * e2e_steps * paths_per_step / (float(t2.item()) * 1e-3) / 1e6
+    e2e_value = world * e2e_blocks * B * paths_per_step / (float(t2.item()) * 1e-3) / 1e6
 
     launches_per_step = 1 if args.kernel == "mega" else 2 + 2 * cfg.max_path_length
     if use_bundles:
-        launches_per_step = 1.0 / B
+        # a bundle: one megakernel launch, or the loop's init kernel plus three kernels per iteration
+        launches_per_step = (1.0 + 3 * loop_iters if wave_loop else 1.0) / B
     peak, peak_src = measured_peak()
     step_s = ms_max * 1e-3 / args.steps
     achieved = bytes_per_path * paths_per_step / step_s / 1e9
-    traffic = profiled_traffic(args.kernel, args.workload, args.width, args.occupancy, use_bundles)
+    traffic = profiled_traffic(args.kernel, args.workload, args.width, 0 if wave_loop else args.occupancy,
+                               use_bundles)
 
     line = {"metric": "Mpaths/s", "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded procedural scene; no dataset)",
             "config": {"workload": desc, "kernel": args.kernel, "bvh_width": args.width, "traversal": args.traversal,
-                       "occupancy": args.occupancy,
-                       "launches": ("one launch per 25-pass wavelength bundle (each pass its own band, the same "
-                                    "paths as one launch per pass)" if use_bundles else "one launch per pass"),
+                       "occupancy": args.occupancy, "queue_capacity": cfg.queue_capacity,
+                       "launches": (("one regenerating wavefront loop per 25-pass wavelength bundle (init kernel, "
+                                     "then a CUDA-graph while-loop of trace, shade, control; %d iterations)"
+                                     % loop_iters if wave_loop else
+                                     "one launch per 25-pass wavelength bundle") +
+                                    " (each pass its own band, the same paths as one launch per pass)"
+                                    if use_bundles else "one launch per pass"),
                        "paths_per_step": paths_per_step,
                        "spp": ex["spp"], "passes_for_spp": cfg.samples_per_pixel,
                        "l2": "inputs larger than L2: scene %.0f MB + film %.0f MB > 126 MB L2; no flush"
@@ -580,13 +605,17 @@ def bench_ours(args):
                                 paths_per_step * B * 8 / 1e6),
                        "parallelism": f"{world} GPU(s), disjoint sample passes per GPU"},
             "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": 36,
-                    "d2h_bytes_per_step": int(out.nbytes),
-                    "what": "Renderer.update_camera + cast_rays + resolve_xyz_host (pinned host XYZ image) per "
-                            "step, through the C ABI"},
+                    "d2h_bytes_per_step": int(out.nbytes), "passes_per_step": B,
+                    "what": "per step (one spectral block): Renderer.update_camera + %s + "
+                            "average_and_reset_block + resolve_xyz_host (pinned host XYZ image), through the C ABI"
+                            % ("cast_rays_bundle of the block's %d passes" % B if use_bundles
+                               else "%d cast_rays" % B)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "traffic_per": "pass (ncu capture of a launch of the same configuration, per pass)",
-                         "kernel": "k_render_mega" if args.kernel == "mega" else "wavefront pass",
+                         "kernel": ("k_render_mega" if args.kernel == "mega" else
+                                    "wavefront loop (k_trace + k_shade_loop + k_loop_control per iteration)"
+                                    if wave_loop else "wavefront pass"),
                          "bytes_per_path": bytes_per_path, "peak_source": peak_src,
                          "work_per_path": {k: v / work["paths"] for k, v in work.items() if k != "paths"}},
             "gpu_launches": int(round(launches_per_step * args.steps + (args.steps % B if use_bundles else 0))),
@@ -609,7 +638,7 @@ def bench_ours(args):
     if rank == 0 and world == 1 and not args.no_extras:
         # the plain single-scene wavefront kernel on the same workload (same paths)
         r.set_launch_config(kernel="wavefront", traversal="default", block_size=128, blocks_per_sm=0, sort_keys=0,
-                            trace_budget=16, occupancy=0)
+                            trace_budget=16, occupancy=0, queue_capacity=0)
         for k in range(3):
             r.cast_rays(k % B, pass_idx=base_pass + 9000 + k)
         torch.cuda.synchronize()

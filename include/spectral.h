@@ -63,8 +63,12 @@ typedef struct {
   int32_t traversal;             /* TS_TRAVERSAL_DEFAULT or TS_TRAVERSAL_SPECULATIVE (two-child nodes) */
   int32_t occupancy;             /* megakernel register budget: 0 = 5 resident blocks of 128 per SM (96 registers),
                                     8 = 8 blocks (64 registers, spills; more latency hiding on large frames) */
-  int32_t queue_capacity;        /* wavefront: paths per chunk of the frame (0 = whole frame); the queues and
-                                    path state of one chunk are allocated, so a small capacity keeps them in L2 */
+  int32_t queue_capacity;        /* wavefront path slots (0 = one per pixel; at most 2^25).  With sort_keys == 0,
+                                    ts_render_passes, and ts_render_pass when queue_capacity > 0, run the
+                                    regenerating loop: a slot whose path has ended starts the next pixel (of
+                                    the next pass of a bundle) at once, so several passes can be in flight.
+                                    With sort_keys != 0 a pass is rendered depth-synchronously in chunks of at
+                                    most queue_capacity pixels. */
 } ts_config;
 
 /* Scene in the reference's data model (setup_scene, main.py:509-631). Triangles
@@ -142,8 +146,14 @@ ts_status ts_render_pass(ts_ctx *ctx, uint32_t pass_idx, int32_t band, void *str
  * that every pass owns its own film plane; the same paths and deposits as
  * num_passes ts_render_pass calls (film sums equal up to the order of FP64
  * additions where volume fluorescence moves deposits between bands).  Small frames fill the GPU this way.  The
- * wavefront kernel falls back to one launch per pass. */
+ * wavefront kernel runs it as the regenerating loop (sort_keys == 0: one init kernel, then a CUDA graph
+ * whose while-loop iterates trace -> shade until the queues are empty), or one depth-synchronous launch
+ * sequence per pass (sort_keys != 0). */
 ts_status ts_render_passes(ts_ctx *ctx, uint32_t first_pass, int32_t num_passes, int32_t first_band, void *stream);
+
+/* Loop iterations of the last regenerating wavefront launch (each one trace,
+ * one shade and one control kernel); synchronises the stream.  0 before any. */
+ts_status ts_wave_loop_iterations(ts_ctx *ctx, void *stream, int32_t *iterations);
 
 /* The same pass rendered by the plain megakernel with work counters (used to
  * derive algorithmic bytes per path).  work[0..6] = paths, path vertices,

@@ -9,8 +9,9 @@ only its cost.  Knobs:
   * traversal loop of two-child nodes (default if-if / speculative while-while),
   * kernel: the persistent megakernel or the wavefront stages, and for the
     wavefront its queue sorting (sort_keys bit mask), the traversal steps
-    between lane refills (trace_budget) and the queue capacity (paths per
-    chunk of the frame),
+    between lane refills (trace_budget) and, for wavelength bundles, the
+    queue capacity of the regenerating loop (path slots: how many passes'
+    paths are in flight at once),
   * threads per block and resident blocks per SM of the persistent grid, and
     the megakernel's register budget (5 blocks/SM without spills, or 8 with).
 
@@ -61,9 +62,18 @@ def default_candidates(quick=False):
     if not quick:
         out += [Candidate(w, "default", "wavefront", 128, 0, sk, tb)
                 for w in (2, 4) for sk in (0, 1) for tb in (16, 32, 64)]
-        out += [Candidate(w, "default", "wavefront", 128, 0, 0, 16, queue_capacity=qc)
-                for w in (2, 4) for qc in (1 << 16, 1 << 18)]
     return out
+
+
+MAX_QUEUE_CAPACITY = 1 << 25
+
+
+def bundle_wavefront_candidates(npix, bands, widths=(2, 4), multiples=(2, 4, 8, 16, 32)):
+    """Regenerating-loop wavefront candidates for wavelength bundles: queue
+    capacities of several frames' worth of path slots (passes in flight),
+    up to the whole bundle."""
+    caps = sorted({min(m * npix, bands * npix, MAX_QUEUE_CAPACITY) for m in multiples})
+    return [Candidate(w, "default", "wavefront", 128, 0, 0, 16, queue_capacity=qc) for w in widths for qc in caps]
 
 
 def signature(compiled, cfg, bundles=False):
@@ -106,8 +116,11 @@ def tune(scene_dict, cfg, eems=None, cmf=None, candidates=None, passes=6, warmup
          first_pass=1 << 24, bundles=False):
     """Time every candidate on this scene; returns (best Candidate, [(Candidate, ms per pass)]).
 
-    bundles: time whole-block launches (cast_rays_bundle, megakernel candidates only)
-    instead of one launch per pass -- the two favour different block shapes."""
+    bundles: time whole-block launches (cast_rays_bundle) instead of one launch
+    per pass -- the two favour different block shapes.  Bundles are timed for
+    the megakernel candidates and for the regenerating wavefront loop over a
+    range of queue capacities (sorted-queue wavefront candidates are dropped:
+    they launch per pass)."""
     compiled = compile_scene(scene_dict, cfg.bands, eems=eems, cmf=cmf)
     key = signature(compiled, cfg, bundles)
     if cache and os.path.exists(cache):
@@ -118,7 +131,9 @@ def tune(scene_dict, cfg, eems=None, cmf=None, candidates=None, passes=6, warmup
     bvh = _lib.build_bvh_host(compiled.tris["v0"], compiled.tris["v1"], compiled.tris["v2"])
     candidates = list(candidates or default_candidates(quick))
     if bundles:
-        candidates = [c for c in candidates if c.kernel == "mega"]
+        candidates = [c for c in candidates if c.kernel == "mega" or c.sort_keys == 0]
+        extra = bundle_wavefront_candidates(cfg.width * cfg.height, cfg.bands)
+        candidates += [c for c in extra if c not in candidates]
     table = []
     for width in sorted({c.width for c in candidates}):
         group = [c for c in candidates if c.width == width]

@@ -565,6 +565,18 @@ ts_status ts_render_passes(ts_ctx *c, uint32_t first_pass, int32_t num_passes, i
   return TS_OK;
 }
 
+ts_status ts_wave_loop_iterations(ts_ctx *c, void *stream, int32_t *iterations) {
+  if (!c || !iterations) return fail(c, TS_ERR_INVALID_ARG, "ts_wave_loop_iterations: null argument");
+  *iterations = 0;
+  if (!c->wave_loop || !c->wave.loop) return TS_OK;
+  cudaSetDevice(c->cfg.device);
+  const cudaStream_t st = as_stream(stream);
+  TS_CUDA(c, cudaMemcpyAsync(iterations, &c->wave.loop->iter, sizeof(int32_t), cudaMemcpyDeviceToHost, st),
+          "ts_wave_loop_iterations");
+  TS_CUDA(c, cudaStreamSynchronize(st), "ts_wave_loop_iterations");
+  return TS_OK;
+}
+
 ts_status ts_render_pass_counted(ts_ctx *c, uint32_t pass_idx, int32_t band, void *stream, uint64_t work[8]) {
   if (!c || !work) return fail(c, TS_ERR_INVALID_ARG, "ts_render_pass_counted: bad argument");
   if (!c->has_scene) return fail(c, TS_ERR_NO_SCENE, "ts_render_pass_counted: no scene uploaded");
@@ -1001,6 +1013,7 @@ static ts_status ensure_wave(ts_ctx *c) {
   TS_CUDA(c, grab((void **)&w.key_hist, 2 * ts::kMaxKeys * sizeof(int)), "wavefront buffers");
   TS_CUDA(c, grab((void **)&w.tag, N * sizeof(int)), "wavefront buffers");
   TS_CUDA(c, grab((void **)&w.loop, sizeof(ts::WaveLoop)), "wavefront buffers");
+  TS_CUDA(c, cudaMemset(w.loop, 0, sizeof(ts::WaveLoop)), "wavefront buffers");
   w.capacity = n;
   return TS_OK;
 }

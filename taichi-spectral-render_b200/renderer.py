@@ -214,6 +214,12 @@ class Renderer:
                                               int(first_band), _stream()))
         self.total_samples += int(num_passes)
 
+    def wave_loop_iterations(self):
+        """Iterations (trace + shade + control launches) of the last regenerating wavefront launch."""
+        n = ctypes.c_int32(0)
+        self._check(self.lib.ts_wave_loop_iterations(self._ctx, _stream(), ctypes.byref(n)))
+        return int(n.value)
+
     def cast_rays_counted(self, current_sample_in_block, pass_idx=None):
         """cast_rays through the counting megakernel; returns the work counts."""
         if pass_idx is None:

@@ -110,8 +110,10 @@ def test_wavefront_equals_megakernel():
 
 
 def test_wavefront_queue_capacity_changes_no_result():
-    """A pass rendered in chunks of the frame (ragged last chunk included) deposits
-    the same paths into the same cells as a whole-frame pass."""
+    """A pass over queue_capacity path slots -- the regenerating loop (unsorted
+    queues), or depth-synchronous chunks of the frame with a ragged last chunk
+    (sorted queues) -- deposits the same paths into the same cells as a
+    whole-frame pass."""
     s, c, ex, comp, bvh = setup(configs.volume_scene, width=64, height=64, medium_slices=30, medium_stacks=31,
                                 fluorescent_medium=True)
     passes = range(10)
@@ -128,6 +130,8 @@ def test_wavefront_queue_capacity_changes_no_result():
             r.cast_rays(p % c.bands, pass_idx=p)
         g = r.block_film.cpu().numpy().reshape(c.bands, -1).T.copy()
         assert r.check_device() == 0
+        # 64*64 pixels over 513 slots: at least 8 slot generations of iterations
+        assert 8 <= r.wave_loop_iterations() <= (64 * 64 // 513 + 3) * (c.max_path_length + 1) + 4
     assert np.array_equal(whole, g)
 
 
