@@ -182,19 +182,24 @@ struct PathState {
   int active, active_px, plen, vol;
 };
 
-// camera ray of cast_rays, main.py:1505-1529 (fov_scale = 1 is the reference)
-TS_D void camera_ray(const DevScene &s, const DevConfig &c, int i, int j, Rng &rng, PathState &p, int band) {
+// camera ray of cast_rays, main.py:1505-1529 (fov_scale = 1 is the reference),
+// from the camera origin o and basis (cu, cv, cw)
+TS_D void camera_ray(float3 o, float3 cu, float3 cv, float3 cw, const DevConfig &c, int i, int j, Rng &rng,
+                     PathState &p, int band) {
   const float u = ((float)i + rng.next()) / (float)c.W;
   const float v = ((float)j + rng.next()) / (float)c.H;
-  p.dir = normalize(s.cam_u * ((u * 2.0f - 1.0f) * c.aspect * c.fov) + s.cam_v * ((v * 2.0f - 1.0f) * c.fov) -
-                    s.cam_w * 2.0f);
-  p.pos = s.cam_o;
+  p.dir = normalize(cu * ((u * 2.0f - 1.0f) * c.aspect * c.fov) + cv * ((v * 2.0f - 1.0f) * c.fov) - cw * 2.0f);
+  p.pos = o;
   p.thr = 1.0f;
   p.spdf = 1.0f;
   p.active = band;
   p.active_px = band;
   p.plen = 0;
   p.vol = 0;
+}
+
+TS_D void camera_ray(const DevScene &s, const DevConfig &c, int i, int j, Rng &rng, PathState &p, int band) {
+  camera_ray(s.cam_o, s.cam_u, s.cam_v, s.cam_w, c, i, j, rng, p, band);
 }
 
 struct VolEvent {

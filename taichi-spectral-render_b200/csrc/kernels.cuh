@@ -46,6 +46,7 @@ struct WaveLoop {
   int iter, limit;
   uint32_t pass0;
   int band0, shared, pad_;
+  float3 cam_o, cam_u, cam_v, cam_w;  // the camera of the launch (not captured in the loop graph)
 };
 
 struct WaveBuffers {

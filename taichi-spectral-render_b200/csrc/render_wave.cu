@@ -65,12 +65,12 @@ __device__ __forceinline__ void deposit(const Film &f, int pixel, int band, floa
 }
 
 // the camera ray of one pixel into path slot `slot` (the pixel id keys the random stream)
-__device__ __forceinline__ void start_path(const DevScene &s, const DevConfig &c, uint32_t pass, int band, int pix,
-                                           const WaveBuffers &w, int slot) {
+__device__ __forceinline__ void start_path(float3 o, float3 cu, float3 cv, float3 cw, const DevConfig &c,
+                                           uint32_t pass, int band, int pix, const WaveBuffers &w, int slot) {
   Rng rng;
   rng.init(c.seed, pass, (uint32_t)pix, c.scene_id);
   PathState ps;
-  camera_ray(s, c, pix % c.W, pix / c.W, rng, ps, band);
+  camera_ray(o, cu, cv, cw, c, pix % c.W, pix / c.W, rng, ps, band);
   w.pos_thr[slot] = make_float4(ps.pos.x, ps.pos.y, ps.pos.z, ps.thr);
   w.dir_spdf[slot] = make_float4(ps.dir.x, ps.dir.y, ps.dir.z, ps.spdf);
   w.meta[slot] = make_int4(pix, band | (band << 8), 0, (int)rng.n);
@@ -79,7 +79,7 @@ __device__ __forceinline__ void start_path(const DevScene &s, const DevConfig &c
 // camera rays of pixels [p0, p0 + n): path slot q <-> pixel p0 + q
 __global__ void k_generate(DevScene s, DevConfig c, uint32_t pass, int band, WaveBuffers w, int p0, int n) {
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-    start_path(s, c, pass, band, p0 + q, w, q);
+    start_path(s.cam_o, s.cam_u, s.cam_v, s.cam_w, c, pass, band, p0 + q, w, q);
     w.queue[0][q] = q;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) w.counts[kCntExt + 0] = n;
@@ -407,7 +407,7 @@ __global__ void k_loop_init(DevScene s, DevConfig c, WaveBuffers w, WaveLoop *L,
     const int po = q / npix;
     int band = band0 + po;
     if (band >= c.B) band -= c.B;
-    start_path(s, c, pass0 + (uint32_t)po, band, q - po * npix, w, q);
+    start_path(s.cam_o, s.cam_u, s.cam_v, s.cam_w, c, pass0 + (uint32_t)po, band, q - po * npix, w, q);
     w.tag[q] = po << 16;
     w.queue[0][q] = q;
   }
@@ -423,6 +423,10 @@ __global__ void k_loop_init(DevScene s, DevConfig c, WaveBuffers w, WaveLoop *L,
     L->pass0 = pass0;
     L->band0 = band0;
     L->shared = shared;
+    L->cam_o = s.cam_o;
+    L->cam_u = s.cam_u;
+    L->cam_v = s.cam_v;
+    L->cam_w = s.cam_w;
   }
 }
 
@@ -465,7 +469,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_shade_loop(DevScene s, DevConfig 
         const int po = item / npix;
         int band = band0 + po;
         if (band >= c.B) band -= c.B;
-        start_path(s, c, pass0 + (uint32_t)po, band, item - po * npix, w, pid);
+        start_path(L->cam_o, L->cam_u, L->cam_v, L->cam_w, c, pass0 + (uint32_t)po, band, item - po * npix, w, pid);
         w.tag[pid] = po << 16;
         fresh = true;
       }
@@ -626,6 +630,11 @@ cudaError_t launch_wave_loop(const DevScene &s, const DevConfig &c, uint32_t pas
   } k;
   memset(&k, 0, sizeof k);
   memcpy(&k.s, &s, sizeof s);
+  // the loop kernels take the camera from the loop state: moving it needs no new graph
+  memset(&k.s.cam_o, 0, sizeof k.s.cam_o);
+  memset(&k.s.cam_u, 0, sizeof k.s.cam_u);
+  memset(&k.s.cam_v, 0, sizeof k.s.cam_v);
+  memset(&k.s.cam_w, 0, sizeof k.s.cam_w);
   memcpy(&k.c, &c, sizeof c);
   memcpy(&k.f, &f, sizeof f);
   memcpy(&k.w, &w, sizeof w);

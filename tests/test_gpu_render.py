@@ -183,6 +183,28 @@ def test_wavefront_regenerating_loop_bundles():
     assert np.array_equal(per_pass, gpu_bundles(s, c, ex, bvh, "wavefront", [(0, 0, 25)], sort_keys=1))
 
 
+def test_wavefront_loop_follows_the_camera():
+    """The captured loop takes the camera from its launch: a moved camera
+    needs no new graph and renders the moved view."""
+    s, c, ex, comp, bvh = setup(configs.box_scene, width=48, height=48)
+    cam = s["camera"]
+    moved = np.asarray(cam["origin"], np.float64) + np.array([0.35, -0.2, 0.1])
+    films = []
+    for bundle in (True, False):
+        c2 = sb.RenderConfig(**{**c.__dict__, "kernel": "wavefront", "queue_capacity": 3 * 48 * 48})
+        with sb.Renderer(s, c2, eems=ex["eems"], cmf=ex["cmf"], bvh=bvh) as r:
+            for blk, origin in enumerate((cam["origin"], moved, cam["origin"])):
+                r.update_camera(origin, cam["lookat"], cam["up"])
+                if bundle:
+                    r.cast_rays_bundle(0, c.bands, pass_idx=blk * c.bands)
+                else:
+                    for b in range(c.bands):
+                        r.cast_rays(b, pass_idx=blk * c.bands + b)
+            films.append(r.block_film.cpu().numpy())
+            assert r.check_device() == 0
+    assert np.array_equal(films[0], films[1])
+
+
 def test_statistical_parity_three_sigma():
     """Independent streams: per-cell means agree within 3 combined standard errors."""
     s, c, ex, comp, bvh = setup(configs.box_scene, width=16, height=16)
