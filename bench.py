@@ -49,6 +49,8 @@ def parse():
     p.add_argument("--budget", type=int, default=0, help="wavefront traversal steps between refills")
     p.add_argument("--queue-capacity", type=int, default=0,
                    help="wavefront path slots of the regenerating loop (--no-tune; 0 = one per pixel)")
+    p.add_argument("--loop-host", action="store_true",
+                   help="launch the wavefront loop's iterations from the host (for kernel profilers)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-extras", action="store_true", help="skip the time-to-RMSE and adjoint-cost legs")
     p.add_argument("--no-tune", action="store_true", help="use --kernel/--width/--traversal as given instead of "
@@ -476,6 +478,7 @@ def bench_ours(args):
     cfg.trace_budget = args.budget
     cfg.occupancy = args.occupancy
     cfg.queue_capacity = args.queue_capacity
+    cfg.loop_host = 1 if args.loop_host else 0
     cfg.device = local
     tuned = None
     if not args.no_tune:

@@ -69,6 +69,10 @@ typedef struct {
                                     the next pass of a bundle) at once, so several passes can be in flight.
                                     With sort_keys != 0 a pass is rendered depth-synchronously in chunks of at
                                     most queue_capacity pixels. */
+  int32_t loop_host;             /* regenerating loop: 0 = the iterations run as a CUDA-graph while-loop;
+                                    1 = the host launches them, reading the loop's continue flag after each
+                                    (one stream synchronisation per iteration: for profilers that do not
+                                    descend into conditional graph nodes).  Results are identical. */
 } ts_config;
 
 /* Scene in the reference's data model (setup_scene, main.py:509-631). Triangles
@@ -111,7 +115,7 @@ typedef struct {
 ts_status ts_create(const ts_config *cfg, ts_ctx **out);
 ts_status ts_destroy(ts_ctx *ctx);
 /* Change the launch settings of a context -- kernel, traversal, block_size,
- * blocks_per_sm, sort_keys, trace_budget, occupancy, queue_capacity of *cfg; every other field is
+ * blocks_per_sm, sort_keys, trace_budget, occupancy, queue_capacity, loop_host of *cfg; every other field is
  * ignored -- without re-uploading the scene (the autotuner's knob).  Paths and
  * images do not depend on these settings. */
 ts_status ts_set_launch_config(ts_ctx *ctx, const ts_config *cfg);

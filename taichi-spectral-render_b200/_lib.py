@@ -37,7 +37,7 @@ class TsConfig(ctypes.Structure):
                 ("device", ctypes.c_int32), ("kernel", ctypes.c_int32), ("block_size", ctypes.c_int32),
                 ("blocks_per_sm", ctypes.c_int32), ("sort_keys", ctypes.c_int32), ("trace_budget", ctypes.c_int32),
                 ("traversal", ctypes.c_int32), ("occupancy", ctypes.c_int32),
-                ("queue_capacity", ctypes.c_int32)]
+                ("queue_capacity", ctypes.c_int32), ("loop_host", ctypes.c_int32)]
 
 
 class TsSceneDesc(ctypes.Structure):

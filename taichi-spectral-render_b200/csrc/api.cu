@@ -215,6 +215,7 @@ ts_status ts_set_launch_config(ts_ctx *c, const ts_config *k) {
   if (k->queue_capacity > kMaxQueueCapacity)
     return fail(c, TS_ERR_INVALID_ARG, "ts_set_launch_config: queue_capacity above 2^25 path slots");
   c->cfg.queue_capacity = k->queue_capacity;
+  c->cfg.loop_host = k->loop_host;
   c->dc.speculative = k->traversal == TS_TRAVERSAL_SPECULATIVE ? 1 : 0;
   return TS_OK;
 }
@@ -499,7 +500,8 @@ static ts_status render_wave_loop(ts_ctx *c, uint32_t pass0, int npass, int band
   int per_sm = c->cfg.blocks_per_sm;
   if (per_sm <= 0) per_sm = std::max(1, 2048 / bs);
   TS_CUDA(c, ts::launch_wave_loop(c->ds, c->dc, pass0, band0, npass, film_of(c), c->wave, c->d_err,
-                                  c->num_sms * per_sm, bs, st, c->cfg.trace_budget, cap, &c->wave_loop),
+                                  c->num_sms * per_sm, bs, st, c->cfg.trace_budget, cap, &c->wave_loop,
+                                  c->cfg.loop_host != 0),
           what);
   return TS_OK;
 }

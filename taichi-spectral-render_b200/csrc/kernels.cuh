@@ -47,6 +47,7 @@ struct WaveLoop {
   uint32_t pass0;
   int band0, shared, pad_;
   float3 cam_o, cam_u, cam_v, cam_w;  // the camera of the launch (not captured in the loop graph)
+  int go;                             // continue flag of the last iteration
 };
 
 struct WaveBuffers {
@@ -81,9 +82,10 @@ cudaError_t launch_wave_pass(const DevScene &s, const DevConfig &c, uint32_t pas
 // slots (<= w.capacity) with path regeneration, as a CUDA-graph while-loop.
 // *graph caches the captured loop (rebuilt when a captured argument changes).
 struct WaveLoopGraph;
+// host_driven: launch the iterations from the host instead (one stream sync each)
 cudaError_t launch_wave_loop(const DevScene &s, const DevConfig &c, uint32_t pass0, int band0, int npass, Film f,
                              const WaveBuffers &w, uint32_t *err, int grid, int block, cudaStream_t st,
-                             int trace_budget, int capacity, WaveLoopGraph **graph);
+                             int trace_budget, int capacity, WaveLoopGraph **graph, bool host_driven = false);
 void free_wave_loop(WaveLoopGraph *graph);
 
 // ---- path-replay adjoint (adjoint.cu) -----------------------------------------

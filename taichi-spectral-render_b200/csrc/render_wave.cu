@@ -482,7 +482,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_shade_loop(DevScene s, DevConfig 
 // end of an iteration: go on while rays or shadow queries are queued, reset
 // the counters the next iteration appends to, and stop (with an error bit) at
 // the iteration bound, which no launch reaches unless the queues are corrupt
-__global__ void k_loop_control(WaveLoop *L, cudaGraphConditionalHandle h, uint32_t *err) {
+__global__ void k_loop_control(WaveLoop *L, cudaGraphConditionalHandle h, int in_graph, uint32_t *err) {
   if (threadIdx.x != 0) return;
   const int a = L->iter & 1;
   bool go = L->ext[a ^ 1] > 0 || L->sh[a] > 0;
@@ -495,7 +495,8 @@ __global__ void k_loop_control(WaveLoop *L, cudaGraphConditionalHandle h, uint32
     atomicOr(err, kErrIterationCap);
     go = false;
   }
-  cudaGraphSetConditional(h, go ? 1u : 0u);
+  L->go = go ? 1 : 0;
+  if (in_graph) cudaGraphSetConditional(h, go ? 1u : 0u);
 }
 
 }  // namespace
@@ -594,7 +595,7 @@ cudaError_t build_wave_loop(WaveLoopGraph &G, const DevScene &s, const DevConfig
     return e;
   launch_trace<true>(s, c, 0, f, w, err, grid, block, G.capture, budget, 0, 0, w.loop);
   k_shade_loop<<<grid, block, 0, G.capture>>>(s, c, f, w, w.loop);
-  k_loop_control<<<1, 32, 0, G.capture>>>(w.loop, h, err);
+  k_loop_control<<<1, 32, 0, G.capture>>>(w.loop, h, 1, err);
   const cudaError_t le = cudaGetLastError();
   cudaGraph_t captured = nullptr;
   e = cudaStreamEndCapture(G.capture, &captured);
@@ -607,7 +608,7 @@ cudaError_t build_wave_loop(WaveLoopGraph &G, const DevScene &s, const DevConfig
 
 cudaError_t launch_wave_loop(const DevScene &s, const DevConfig &c, uint32_t pass0, int band0, int npass, Film f,
                              const WaveBuffers &w, uint32_t *err, int grid, int block, cudaStream_t st,
-                             int trace_budget, int capacity, WaveLoopGraph **graph) {
+                             int trace_budget, int capacity, WaveLoopGraph **graph, bool host_driven) {
   const int64_t npix = (int64_t)c.W * c.H;
   const int64_t total = npix * npass;
   if (c.max_depth > kMaxDepth || npass < 1 || npass > 32767 || capacity < 1 || capacity > w.capacity ||
@@ -643,6 +644,21 @@ cudaError_t launch_wave_loop(const DevScene &s, const DevConfig &c, uint32_t pas
   k.block = block;
   k.budget = trace_budget;
   const unsigned char *kb = reinterpret_cast<const unsigned char *>(&k);
+  if (host_driven) {
+    const int init_grid = (int)((n0 + 255) / 256 < 4096 ? (n0 + 255) / 256 : 4096);
+    k_loop_init<<<init_grid, 256, 0, st>>>(s, c, w, w.loop, pass0, band0, npass, n0, limit, shared);
+    for (int it = 0; it < limit; ++it) {
+      launch_trace<true>(s, c, 0, f, w, err, grid, block, st, trace_budget, 0, 0, w.loop);
+      k_shade_loop<<<grid, block, 0, st>>>(s, c, f, w, w.loop);
+      k_loop_control<<<1, 32, 0, st>>>(w.loop, 0, 0, err);
+      int go = 0;
+      cudaError_t e = cudaMemcpyAsync(&go, &w.loop->go, sizeof(int), cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+      if (e != cudaSuccess) return e;
+      if (!go) break;
+    }
+    return cudaGetLastError();
+  }
   if (!*graph) *graph = new WaveLoopGraph;
   WaveLoopGraph &G = **graph;
   if (!G.exec || G.key.size() != sizeof k || memcmp(G.key.data(), kb, sizeof k) != 0) {

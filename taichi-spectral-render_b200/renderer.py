@@ -56,7 +56,8 @@ class RenderConfig:
     trace_budget: int = 0
     traversal: str = "default"      # two-child nodes: "default" (if-if loop) or "speculative" (while-while)
     occupancy: int = 0              # megakernel: 0 = 5 blocks/SM (96 registers), 8 = 8 blocks/SM (64 registers)
-    queue_capacity: int = 0         # wavefront: paths per chunk of the frame (0 = whole frame)
+    queue_capacity: int = 0         # wavefront path slots (0 = one per pixel); see ts_config
+    loop_host: int = 0              # wavefront loop iterations launched by the host (profiling)
     device: int = 0
 
     @property
@@ -80,6 +81,7 @@ class RenderConfig:
         c.traversal = {"default": 0, "speculative": 1}[self.traversal]
         c.occupancy = self.occupancy
         c.queue_capacity = self.queue_capacity
+        c.loop_host = self.loop_host
         return c
 
 
@@ -144,12 +146,13 @@ class Renderer:
         _lib.check(status, self._ctx)
 
     def set_launch_config(self, kernel=None, traversal=None, block_size=None, blocks_per_sm=None, sort_keys=None,
-                          trace_budget=None, occupancy=None, queue_capacity=None):
+                          trace_budget=None, occupancy=None, queue_capacity=None, loop_host=None):
         """Change launch settings without re-uploading the scene (images do not depend on them)."""
         upd = {k: v for k, v in dict(kernel=kernel, traversal=traversal, block_size=block_size,
                                      blocks_per_sm=blocks_per_sm, sort_keys=sort_keys,
                                      trace_budget=trace_budget, occupancy=occupancy,
-                                     queue_capacity=queue_capacity).items() if v is not None}
+                                     queue_capacity=queue_capacity, loop_host=loop_host).items()
+               if v is not None}
         cfg = dataclasses.replace(self.config, **upd)
         self._check(self.lib.ts_set_launch_config(self._ctx, ctypes.byref(cfg.to_c())))
         self.config = cfg

@@ -135,10 +135,10 @@ def test_wavefront_queue_capacity_changes_no_result():
     assert np.array_equal(whole, g)
 
 
-def gpu_bundles(scene, cfg, ex, bvh, kernel, bundles, queue_capacity=0, sort_keys=0):
+def gpu_bundles(scene, cfg, ex, bvh, kernel, bundles, queue_capacity=0, sort_keys=0, loop_host=0):
     """(first_pass, first_band, num_passes) launches into one film."""
     c2 = sb.RenderConfig(**{**cfg.__dict__, "kernel": kernel, "queue_capacity": queue_capacity,
-                            "sort_keys": sort_keys})
+                            "sort_keys": sort_keys, "loop_host": loop_host})
     with sb.Renderer(scene, c2, eems=ex["eems"], cmf=ex["cmf"], bvh=bvh) as r:
         for p0, b0, n in bundles:
             r.cast_rays_bundle(b0, n, pass_idx=p0)
@@ -167,6 +167,9 @@ def test_wavefront_regenerating_loop_bundles():
     for cap in (0, 500, 3 * 48 * 48):
         g = gpu_bundles(s, c, ex, bvh, "wavefront", [(0, 0, 25), (25, 0, 25)], queue_capacity=cap)
         assert np.array_equal(per_pass, g), cap
+    # iterations launched from the host instead of the graph's while-loop
+    g = gpu_bundles(s, c, ex, bvh, "wavefront", [(0, 0, 25), (25, 0, 25)], queue_capacity=500, loop_host=1)
+    assert np.array_equal(per_pass, g)
     # bundles that start mid-block and wrap the band index
     per_pass = gpu_passes(s, c, ex, bvh, "wavefront", range(7, 27))
     assert np.array_equal(per_pass, gpu_bundles(s, c, ex, bvh, "wavefront", [(7, 7, 11), (18, 18, 9)],
