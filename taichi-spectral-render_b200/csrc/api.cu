@@ -570,7 +570,7 @@ ts_status ts_render_passes(ts_ctx *c, uint32_t first_pass, int32_t num_passes, i
 ts_status ts_wave_loop_iterations(ts_ctx *c, void *stream, int32_t *iterations) {
   if (!c || !iterations) return fail(c, TS_ERR_INVALID_ARG, "ts_wave_loop_iterations: null argument");
   *iterations = 0;
-  if (!c->wave_loop || !c->wave.loop) return TS_OK;
+  if (!c->wave.loop) return TS_OK;
   cudaSetDevice(c->cfg.device);
   const cudaStream_t st = as_stream(stream);
   TS_CUDA(c, cudaMemcpyAsync(iterations, &c->wave.loop->iter, sizeof(int32_t), cudaMemcpyDeviceToHost, st),
