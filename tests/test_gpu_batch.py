@@ -135,3 +135,39 @@ def test_batch_rejects_mixed_bvh_widths():
         sbatch.Batch([r1, r2])
     r1.close()
     r2.close()
+
+
+def test_stream_batch_equals_single_scene_renders():
+    """Each scene's block as one regenerating-loop launch on a pool of streams:
+    the films of one launch per pass, whatever BVH widths the scenes have."""
+    args = [make(fn, **kw) for fn, kw in SCENES]
+    refs = [single_scene_mean(a, 3, first_pass=25) for a in args]
+    rs = [renderer(a) for a in args[:2]]
+    s, c, ex, bvh = args[2]
+    rs.append(sb.Renderer(s, c, eems=ex["eems"], cmf=ex["cmf"], bvh=bvh, bvh_params={"width": 4}))
+    with sbatch.StreamBatch(rs, streams=2) as b:
+        b.reset(first_pass=25)
+        for _ in range(3):
+            b.step()
+        assert b.check() == 0
+        for i, (r, (mean, m2)) in enumerate(zip(rs, refs)):
+            assert r.config.kernel == "wavefront" and r.config.queue_capacity > 0
+            if i == 1:  # fluorescent medium
+                assert same_film(r.mean_film, mean) and same_film(r.m2_film, m2)
+            else:
+                assert torch.equal(r.mean_film, mean) and torch.equal(r.m2_film, m2)
+        keep = rs[1].mean_film.clone()
+        b.set_active([True, False, True])
+        b.step()
+        b.synchronize()
+        assert torch.equal(rs[1].mean_film, keep)
+        assert list(b.blocks) == [4, 3, 4]
+        ref4 = single_scene_mean(args[0], 4, first_pass=25)
+        assert torch.equal(rs[0].mean_film, ref4[0])
+        b.reset()
+        blocks, secs = b.render_to_rmse(target=0.05, max_blocks=200)
+        for r, nb in zip(rs, blocks):
+            assert 2 <= nb < 200
+            assert sbatch.relative_rmse_estimate(r, int(nb)) <= 0.05
+    for r in rs:
+        r.close()
