@@ -245,13 +245,21 @@ class Renderer:
         self.total_samples = 0
         self.num_blocks_completed = 0
 
-    def render(self, samples=None, callback=None):
-        """The pass/block cadence of main.py:1826-1837 for ``samples`` passes."""
+    def render(self, samples=None, callback=None, bundles=True):
+        """The pass/block cadence of main.py:1826-1837 for ``samples`` passes:
+        pass k at band k mod B, the block averaged after every B passes (then
+        ``callback(self)``).  bundles: each whole block is one launch
+        (ts_render_passes: the same paths and deposits as B cast_rays calls)."""
         samples = self.config.samples_per_pixel if samples is None else samples
         B = self.config.bands
-        for _ in range(samples):
-            band = self.total_samples % B
-            self.cast_rays(band, self.num_blocks_completed)
+        left = int(samples)
+        while left > 0:
+            if bundles and left >= B and self.total_samples % B == 0:
+                self.cast_rays_bundle(0, B)
+                left -= B
+            else:
+                self.cast_rays(self.total_samples % B, self.num_blocks_completed)
+                left -= 1
             if self.total_samples % B == 0:
                 self.average_and_reset_block(self.num_blocks_completed + 1)
                 if callback is not None:

@@ -208,6 +208,29 @@ def test_wavefront_loop_follows_the_camera():
     assert np.array_equal(films[0], films[1])
 
 
+@pytest.mark.parametrize("kernel,cap", [("mega", 0), ("wavefront", 3 * 24 * 20)])
+def test_render_bundles_whole_blocks(kernel, cap):
+    """Renderer.render launches each whole block as one bundle: the films,
+    counters and callbacks of the pass-by-pass cadence."""
+    s, c, ex, comp, bvh = setup(configs.volume_scene, width=24, height=20, medium_slices=12, medium_stacks=13,
+                                fluorescent_medium=True, depth=8)
+    B = c.bands
+    c2 = sb.RenderConfig(**{**c.__dict__, "kernel": kernel, "queue_capacity": cap})
+    out = []
+    for bundles in (False, True):
+        calls = []
+        with sb.Renderer(s, c2, eems=ex["eems"], cmf=ex["cmf"], bvh=bvh) as r:
+            r.cast_rays(0)  # start off the block boundary: one single pass, then whole blocks
+            r.render(2 * B + 7, callback=lambda rr: calls.append(rr.num_blocks_completed), bundles=bundles)
+            out.append((r.mean_film.clone(), r.m2_film.clone(), r.block_film.clone(), r.total_samples,
+                        r.num_blocks_completed, calls))
+            assert r.check_device() == 0
+    (m0, q0, b0, t0, n0, c0), (m1, q1, b1, t1, n1, c1) = out
+    assert (t0, n0, c0) == (t1, n1, c1) == (2 * B + 8, 2, [1, 2])
+    for a, b in ((m0, m1), (q0, q1), (b0, b1)):
+        assert torch.allclose(a, b, rtol=1e-12, atol=0)
+
+
 def test_statistical_parity_three_sigma():
     """Independent streams: per-cell means agree within 3 combined standard errors."""
     s, c, ex, comp, bvh = setup(configs.box_scene, width=16, height=16)
