@@ -501,7 +501,7 @@ static ts_status render_wave_loop(ts_ctx *c, uint32_t pass0, int npass, int band
   if (per_sm <= 0) per_sm = std::max(1, 2048 / bs);
   TS_CUDA(c, ts::launch_wave_loop(c->ds, c->dc, pass0, band0, npass, film_of(c), c->wave, c->d_err,
                                   c->num_sms * per_sm, bs, st, c->cfg.trace_budget, cap, &c->wave_loop,
-                                  c->cfg.loop_host != 0, c->cfg.occupancy),
+                                  c->cfg.loop_host != 0),
           what);
   return TS_OK;
 }

@@ -82,12 +82,10 @@ cudaError_t launch_wave_pass(const DevScene &s, const DevConfig &c, uint32_t pas
 // slots (<= w.capacity) with path regeneration, as a CUDA-graph while-loop.
 // *graph caches the captured loop (rebuilt when a captured argument changes).
 struct WaveLoopGraph;
-// host_driven: launch the iterations from the host instead (one stream sync each).
-// occupancy: register budget of the trace stage (0 = 64 registers, 5 = 80, 8 = 48)
+// host_driven: launch the iterations from the host instead (one stream sync each)
 cudaError_t launch_wave_loop(const DevScene &s, const DevConfig &c, uint32_t pass0, int band0, int npass, Film f,
                              const WaveBuffers &w, uint32_t *err, int grid, int block, cudaStream_t st,
-                             int trace_budget, int capacity, WaveLoopGraph **graph, bool host_driven = false,
-                             int occupancy = 0);
+                             int trace_budget, int capacity, WaveLoopGraph **graph, bool host_driven = false);
 void free_wave_loop(WaveLoopGraph *graph);
 
 // ---- path-replay adjoint (adjoint.cu) -----------------------------------------

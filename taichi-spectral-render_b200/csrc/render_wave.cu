@@ -90,10 +90,8 @@ __global__ void k_generate(DevScene s, DevConfig c, uint32_t pass, int band, Wav
 // for at most `budget` steps; lanes whose ray has finished then take new work
 // items (one atomic per warp), so a warp does not idle behind its longest ray.
 // kLoop: one iteration of the regenerating loop (queue lengths from *L).
-// kMinBlocks: resident 256-thread blocks per SM the register budget must allow
-// (4: 64 registers; 3: 80, no spills; 5: 48, spills -- more warps in flight).
-template <int W, bool kLoop = false, int kMinBlocks = 4>
-__global__ void __launch_bounds__(kMaxBlock, kMinBlocks) k_trace(DevScene s, DevConfig c, int depth, Film f, WaveBuffers w,
+template <int W, bool kLoop = false>
+__global__ void __launch_bounds__(kMaxBlock, 4) k_trace(DevScene s, DevConfig c, int depth, Film f, WaveBuffers w,
                                                      uint32_t *__restrict__ err, int budget, int ext_sorted,
                                                      int shadow_sorted, WaveLoop *L) {
   uint32_t eb = 0;
@@ -180,30 +178,18 @@ __global__ void __launch_bounds__(kMaxBlock, kMinBlocks) k_trace(DevScene s, Dev
   if (eb) atomicOr(err, eb);
 }
 
-template <bool kLoop = false, int kMinBlocks = 4>
-void launch_trace_b(const DevScene &s, const DevConfig &c, int depth, Film f, const WaveBuffers &w, uint32_t *err,
-                    int grid, int block, cudaStream_t st, int budget, int ext_sorted, int shadow_sorted, WaveLoop *L) {
-  if (s.node_width == 8)
-    k_trace<8, kLoop, kMinBlocks><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget, ext_sorted, shadow_sorted, L);
-  else if (s.node_width == 4)
-    k_trace<4, kLoop, kMinBlocks><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget, ext_sorted, shadow_sorted, L);
-  else if (c.speculative)
-    k_trace<3, kLoop, kMinBlocks><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget, ext_sorted, shadow_sorted, L);
-  else
-    k_trace<2, kLoop, kMinBlocks><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget, ext_sorted, shadow_sorted, L);
-}
-
-// occupancy (the loop's trace stage only): 0 = 64 registers, 5 = 80, 8 = 48
 template <bool kLoop = false>
 void launch_trace(const DevScene &s, const DevConfig &c, int depth, Film f, const WaveBuffers &w, uint32_t *err,
                   int grid, int block, cudaStream_t st, int budget, int ext_sorted = 0, int shadow_sorted = 0,
-                  WaveLoop *L = nullptr, int occupancy = 0) {
-  if (kLoop && occupancy == 5)
-    launch_trace_b<kLoop, 3>(s, c, depth, f, w, err, grid, block, st, budget, ext_sorted, shadow_sorted, L);
-  else if (kLoop && occupancy == 8)
-    launch_trace_b<kLoop, 5>(s, c, depth, f, w, err, grid, block, st, budget, ext_sorted, shadow_sorted, L);
+                  WaveLoop *L = nullptr) {
+  if (s.node_width == 8)
+    k_trace<8, kLoop><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget, ext_sorted, shadow_sorted, L);
+  else if (s.node_width == 4)
+    k_trace<4, kLoop><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget, ext_sorted, shadow_sorted, L);
+  else if (c.speculative)
+    k_trace<3, kLoop><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget, ext_sorted, shadow_sorted, L);
   else
-    launch_trace_b<kLoop, 4>(s, c, depth, f, w, err, grid, block, st, budget, ext_sorted, shadow_sorted, L);
+    k_trace<2, kLoop><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget, ext_sorted, shadow_sorted, L);
 }
 
 // ---- queue sorting ------------------------------------------------------
@@ -586,7 +572,7 @@ void free_wave_loop(WaveLoopGraph *g) {
 namespace {
 
 cudaError_t build_wave_loop(WaveLoopGraph &G, const DevScene &s, const DevConfig &c, Film f, const WaveBuffers &w,
-                            uint32_t *err, int grid, int block, int budget, int occupancy) {
+                            uint32_t *err, int grid, int block, int budget) {
   if (G.exec) cudaGraphExecDestroy(G.exec);
   if (G.graph) cudaGraphDestroy(G.graph);
   G.exec = nullptr;
@@ -607,7 +593,7 @@ cudaError_t build_wave_loop(WaveLoopGraph &G, const DevScene &s, const DevConfig
   if ((e = cudaStreamBeginCaptureToGraph(G.capture, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)) !=
       cudaSuccess)
     return e;
-  launch_trace<true>(s, c, 0, f, w, err, grid, block, G.capture, budget, 0, 0, w.loop, occupancy);
+  launch_trace<true>(s, c, 0, f, w, err, grid, block, G.capture, budget, 0, 0, w.loop);
   k_shade_loop<<<grid, block, 0, G.capture>>>(s, c, f, w, w.loop);
   k_loop_control<<<1, 32, 0, G.capture>>>(w.loop, h, 1, err);
   const cudaError_t le = cudaGetLastError();
@@ -622,8 +608,7 @@ cudaError_t build_wave_loop(WaveLoopGraph &G, const DevScene &s, const DevConfig
 
 cudaError_t launch_wave_loop(const DevScene &s, const DevConfig &c, uint32_t pass0, int band0, int npass, Film f,
                              const WaveBuffers &w, uint32_t *err, int grid, int block, cudaStream_t st,
-                             int trace_budget, int capacity, WaveLoopGraph **graph, bool host_driven,
-                             int occupancy) {
+                             int trace_budget, int capacity, WaveLoopGraph **graph, bool host_driven) {
   const int64_t npix = (int64_t)c.W * c.H;
   const int64_t total = npix * npass;
   if (c.max_depth > kMaxDepth || npass < 1 || npass > 32767 || capacity < 1 || capacity > w.capacity ||
@@ -642,7 +627,7 @@ cudaError_t launch_wave_loop(const DevScene &s, const DevConfig &c, uint32_t pas
     Film f;
     WaveBuffers w;
     uint32_t *err;
-    int grid, block, budget, occupancy;
+    int grid, block, budget;
   } k;
   memset(&k, 0, sizeof k);
   memcpy(&k.s, &s, sizeof s);
@@ -658,13 +643,12 @@ cudaError_t launch_wave_loop(const DevScene &s, const DevConfig &c, uint32_t pas
   k.grid = grid;
   k.block = block;
   k.budget = trace_budget;
-  k.occupancy = occupancy;
   const unsigned char *kb = reinterpret_cast<const unsigned char *>(&k);
   if (host_driven) {
     const int init_grid = (int)((n0 + 255) / 256 < 4096 ? (n0 + 255) / 256 : 4096);
     k_loop_init<<<init_grid, 256, 0, st>>>(s, c, w, w.loop, pass0, band0, npass, n0, limit, shared);
     for (int it = 0; it < limit; ++it) {
-      launch_trace<true>(s, c, 0, f, w, err, grid, block, st, trace_budget, 0, 0, w.loop, occupancy);
+      launch_trace<true>(s, c, 0, f, w, err, grid, block, st, trace_budget, 0, 0, w.loop);
       k_shade_loop<<<grid, block, 0, st>>>(s, c, f, w, w.loop);
       k_loop_control<<<1, 32, 0, st>>>(w.loop, 0, 0, err);
       int go = 0;
@@ -679,7 +663,7 @@ cudaError_t launch_wave_loop(const DevScene &s, const DevConfig &c, uint32_t pas
   WaveLoopGraph &G = **graph;
   if (!G.exec || G.key.size() != sizeof k || memcmp(G.key.data(), kb, sizeof k) != 0) {
     G.key.clear();
-    const cudaError_t e = build_wave_loop(G, s, c, f, w, err, grid, block, trace_budget, occupancy);
+    const cudaError_t e = build_wave_loop(G, s, c, f, w, err, grid, block, trace_budget);
     if (e != cudaSuccess) return e;
     G.key.assign(kb, kb + sizeof k);
   }
