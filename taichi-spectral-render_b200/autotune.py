@@ -73,7 +73,7 @@ def bundle_wavefront_candidates(npix, bands, widths=(2, 4), multiples=(2, 4, 8, 
     capacities of several frames' worth of path slots (passes in flight),
     up to the whole bundle."""
     caps = sorted({min(m * npix, bands * npix, MAX_QUEUE_CAPACITY) for m in multiples})
-    return [Candidate(w, "default", "wavefront", 128, 0, 0, 16, queue_capacity=qc) for w in widths for qc in caps]
+    return [Candidate(w, "default", "wavefront", 256, 0, 0, 16, queue_capacity=qc) for w in widths for qc in caps]
 
 
 def signature(compiled, cfg, bundles=False):

@@ -430,7 +430,9 @@ __global__ void k_loop_init(DevScene s, DevConfig c, WaveBuffers w, WaveLoop *L,
   }
 }
 
-__global__ void __launch_bounds__(kMaxBlock) k_shade_loop(DevScene s, DevConfig c, Film f, WaveBuffers w, WaveLoop *L) {
+// 64 registers (4 resident 256-thread blocks per SM; a few spills): faster
+// than the unbounded 111-register build by 4-6 % on whole-bundle loops
+__global__ void __launch_bounds__(kMaxBlock, 4) k_shade_loop(DevScene s, DevConfig c, Film f, WaveBuffers w, WaveLoop *L) {
   const int a = L->iter & 1;
   const int n = L->ext[a];
   const int *q = w.queue[a];
