@@ -58,3 +58,37 @@ def reduce_gradient(grad, group=None):
         raise TypeError("gradients are reduced in float64")
     dist.all_reduce(grad, group=group)
     return grad
+
+
+def scene_shard(costs, rank, world):
+    """Scenes of a multi-scene batch for ``rank``: scenes are independent, so a
+    batch shards by scene with no exchange in the data path.  Greedy longest-
+    processing-time assignment on estimated costs (e.g. pixels x depth x the
+    blocks a scene needs): scenes by decreasing cost (ties by index), each to
+    the least-loaded rank (ties to the lowest rank).  Every rank computes the
+    same assignment; returns this rank's scene indices in increasing order."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("bad rank/world")
+    costs = [float(c) for c in costs]
+    if any(c < 0 for c in costs):
+        raise ValueError("negative scene cost")
+    load = [0.0] * world
+    mine = []
+    for i in sorted(range(len(costs)), key=lambda k: (-costs[k], k)):
+        r = min(range(world), key=lambda k: (load[k], k))
+        load[r] += costs[i]
+        if r == rank:
+            mine.append(i)
+    return sorted(mine)
+
+
+def gather_scene_blocks(blocks, indices, num_scenes, group=None):
+    """Every rank's per-scene block counts (``blocks[j]`` for scene
+    ``indices[j]``) combined into one int64 vector of ``num_scenes`` entries on
+    every rank (one all-reduce; each scene belongs to exactly one rank)."""
+    import torch.distributed as dist
+    out = torch.zeros(int(num_scenes), dtype=torch.int64)
+    for j, i in enumerate(indices):
+        out[int(i)] = int(blocks[j])
+    dist.all_reduce(out, group=group)
+    return out

@@ -25,6 +25,25 @@ def test_block_range_partitions():
         sd.block_range(4, 2, 2)
 
 
+def test_scene_shard_partitions_and_balances():
+    rng = np.random.default_rng(3)
+    costs = rng.uniform(1, 100, size=37)
+    for world in (1, 2, 3, 8):
+        shards = [sd.scene_shard(costs, r, world) for r in range(world)]
+        flat = sorted(i for s in shards for i in s)
+        assert flat == list(range(len(costs)))  # a partition
+        loads = [costs[s].sum() for s in shards]
+        # greedy LPT: no rank exceeds the mean load by more than the largest scene
+        assert max(loads) <= costs.sum() / world + costs.max() + 1e-9
+        assert shards == [sd.scene_shard(list(costs), r, world) for r in range(world)]  # deterministic
+    # more ranks than scenes: some ranks get none
+    assert [sd.scene_shard([5, 1], r, 3) for r in range(3)] == [[0], [1], []]
+    with pytest.raises(ValueError):
+        sd.scene_shard([1, -1], 0, 1)
+    with pytest.raises(ValueError):
+        sd.scene_shard([1], 1, 1)
+
+
 def _free_port():
     s = socket.socket()
     s.bind(("127.0.0.1", 0))
@@ -95,3 +114,32 @@ def test_reduce_gradient_gloo_world2():
         assert np.allclose(g, want, rtol=1e-13, atol=1e-13)
     with pytest.raises(TypeError):
         sd.reduce_gradient(torch.zeros(3, dtype=torch.float32))
+
+
+def _shard_worker(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    costs = [9, 1, 4, 4, 7, 2]
+    idx = sd.scene_shard(costs, rank, world)
+    blocks = [10 * i + 1 for i in idx]  # a rank's own per-scene results
+    q.put((rank, idx, sd.gather_scene_blocks(blocks, idx, len(costs)).tolist()))
+    dist.destroy_process_group()
+
+
+def test_scene_shard_gather_gloo_world2():
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_shard_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in range(world))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert sorted(res[0][1] + res[1][1]) == list(range(6))
+    # LPT: 9 -> r0, 7 -> r1, 4 -> r1 (7 < 9), 4 -> r0 (9 < 11), 2 -> r1 (11 < 13), 1 -> r0 (13 = 13, lower rank)
+    assert res[0][1] == [0, 1, 3] and res[1][1] == [2, 4, 5]
+    for _, _, gathered in res:
+        assert gathered == [10 * i + 1 for i in range(6)]
