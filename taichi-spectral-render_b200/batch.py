@@ -46,6 +46,8 @@ class Batch:
 
     def __init__(self, renderers, block_size=0, blocks_per_sm=0, use_graph=True, occupancy=0):
         self.renderers = list(renderers)
+        for r in self.renderers:
+            r.flush()
         self.lib = _lib.load()
         n = len(self.renderers)
         arr = (ctypes.c_void_p * n)(*[r._ctx.value for r in self.renderers])
@@ -75,6 +77,8 @@ class Batch:
 
     def reset(self, first_pass=0):
         """Clear every film; the next step renders passes first_pass .. first_pass + B - 1."""
+        for r in self.renderers:
+            r.flush()
         _check(self.lib, self.lib.ts_batch_reset(self._h, int(first_pass) & 0xFFFFFFFF, _stream()), self._h)
         self.blocks[:] = 0
         self.first_pass = int(first_pass)
@@ -90,6 +94,8 @@ class Batch:
 
     def step(self):
         """One spectral block of every active scene, followed by its block average."""
+        for r in self.renderers:
+            r.flush()
         _check(self.lib, self.lib.ts_batch_step(self._h, _stream()), self._h)
         self.blocks[self.active] += 1
         for r, a, nb in zip(self.renderers, self.active, self.blocks):

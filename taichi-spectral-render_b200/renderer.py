@@ -58,6 +58,7 @@ class RenderConfig:
     occupancy: int = 0              # megakernel: 0 = 5 blocks/SM (96 registers), 8 = 8 blocks/SM (64 registers)
     queue_capacity: int = 0         # wavefront path slots (0 = one per pixel); see ts_config
     loop_host: int = 0              # wavefront loop iterations launched by the host (profiling)
+    defer_passes: bool = False      # cast_rays queues passes; runs of consecutive passes launch as bundles
     device: int = 0
 
     @property
@@ -116,6 +117,7 @@ class Renderer:
         self._ctx = ctypes.c_void_p()
         _lib.check(self.lib.ts_create(ctypes.byref(self.config.to_c()), ctypes.byref(self._ctx)))
         self.device = torch.device("cuda", self.config.device)
+        self._pending = []  # deferred (pass_idx, band) of cast_rays, oldest first
         self.total_samples = 0
         self.num_blocks_completed = 0
         self._cam = None
@@ -126,6 +128,7 @@ class Renderer:
 
     # ---------------------------------------------------------------- lifecycle
     def close(self):
+        self._pending = []
         if self._ctx:
             self.lib.ts_destroy(self._ctx)
             self._ctx = ctypes.c_void_p()
@@ -145,9 +148,26 @@ class Renderer:
     def _check(self, status):
         _lib.check(status, self._ctx)
 
+    def flush(self):
+        """Launch the passes that cast_rays deferred (``defer_passes``): one
+        ts_render_passes launch for the run (a single pass: ts_render_pass), on
+        the stream current now.  Every method that touches the film, the scene,
+        the camera or the launch settings flushes first, so deferral changes no
+        result, only how many launches render the passes."""
+        p = getattr(self, "_pending", None)
+        if not p:
+            return
+        self._pending = []
+        first_pass, first_band = p[0]
+        if len(p) == 1:
+            self._check(self.lib.ts_render_pass(self._ctx, first_pass, first_band, _stream()))
+        else:
+            self._check(self.lib.ts_render_passes(self._ctx, first_pass, len(p), first_band, _stream()))
+
     def set_launch_config(self, kernel=None, traversal=None, block_size=None, blocks_per_sm=None, sort_keys=None,
                           trace_budget=None, occupancy=None, queue_capacity=None, loop_host=None):
         """Change launch settings without re-uploading the scene (images do not depend on them)."""
+        self.flush()
         upd = {k: v for k, v in dict(kernel=kernel, traversal=traversal, block_size=block_size,
                                      blocks_per_sm=blocks_per_sm, sort_keys=sort_keys,
                                      trace_budget=trace_budget, occupancy=occupancy,
@@ -160,6 +180,7 @@ class Renderer:
     # ---------------------------------------------------------------- scene
     def setup_scene(self, scene_dict, eems=None, cmf=None, bvh=None, bvh_params=None, exact=None):
         """setup_scene + build_bvh (main.py:437-631): flatten, build the BVH, upload."""
+        self.flush()
         cs = compile_scene(scene_dict, self.config.bands, eems=eems, cmf=cmf, bvh=bvh, bvh_params=bvh_params,
                            exact=exact)
         d = cs.desc()
@@ -187,6 +208,7 @@ class Renderer:
     # ---------------------------------------------------------------- camera
     def update_camera(self, origin=None, lookat=None, up=None):
         """update_camera (main.py:633-640); arguments replace the stored ones."""
+        self.flush()
         o, l, u = self._cam or ([0.0, 0.0, 3.5], [0.0, 0.0, -1.0], [0.0, 1.0, 0.0])
         o = o if origin is None else origin
         l = l if lookat is None else lookat
@@ -201,16 +223,35 @@ class Renderer:
 
         pass_idx picks the random stream; by default it is the number of passes
         rendered since the last clear, so a cleared renderer replays the same
-        sample sequence (common random numbers)."""
+        sample sequence (common random numbers).
+
+        With ``config.defer_passes`` the pass is queued instead: passes that
+        continue the queued run (next pass index, next band mod B) join it, and
+        the run is launched as one wavelength bundle when it holds B passes or
+        when anything else needs the film (``flush``).  The reference's cadence
+        -- B cast_rays, then average_and_reset_block -- then costs one launch
+        per block."""
         if pass_idx is None:
             pass_idx = self.total_samples
-        self._check(self.lib.ts_render_pass(self._ctx, int(pass_idx) & 0xFFFFFFFF, int(current_sample_in_block),
-                                            _stream()))
+        pass_idx = int(pass_idx) & 0xFFFFFFFF
+        band = int(current_sample_in_block)
+        B = self.config.bands
+        if self.config.defer_passes and 0 <= band < B:
+            p = self._pending
+            if p and not (len(p) < B and pass_idx == (p[-1][0] + 1) & 0xFFFFFFFF and band == (p[-1][1] + 1) % B):
+                self.flush()
+            self._pending.append((pass_idx, band))
+            if len(self._pending) == B:
+                self.flush()
+        else:
+            self.flush()
+            self._check(self.lib.ts_render_pass(self._ctx, pass_idx, band, _stream()))
         self.total_samples += 1
 
     def cast_rays_bundle(self, first_band, num_passes, pass_idx=None):
         """num_passes consecutive passes (bands first_band, first_band + 1, ... mod B) in one
         launch: the same paths as num_passes cast_rays calls (num_passes <= bands)."""
+        self.flush()
         if pass_idx is None:
             pass_idx = self.total_samples
         self._check(self.lib.ts_render_passes(self._ctx, int(pass_idx) & 0xFFFFFFFF, int(num_passes),
@@ -219,12 +260,14 @@ class Renderer:
 
     def wave_loop_iterations(self):
         """Iterations (trace + shade + control launches) of the last regenerating wavefront launch."""
+        self.flush()
         n = ctypes.c_int32(0)
         self._check(self.lib.ts_wave_loop_iterations(self._ctx, _stream(), ctypes.byref(n)))
         return int(n.value)
 
     def cast_rays_counted(self, current_sample_in_block, pass_idx=None):
         """cast_rays through the counting megakernel; returns the work counts."""
+        self.flush()
         if pass_idx is None:
             pass_idx = self.total_samples
         w = (ctypes.c_uint64 * 8)()
@@ -236,11 +279,13 @@ class Renderer:
 
     def average_and_reset_block(self, num_blocks_completed):
         """main.py:1592-1607 (FP64 running mean plus the per-cell sum of squares)."""
+        self.flush()
         self._check(self.lib.ts_accumulate_block(self._ctx, int(num_blocks_completed), _stream()))
         self.num_blocks_completed = int(num_blocks_completed)
 
     def clear_pixel_space(self):
         """main.py:1661-1674."""
+        self.flush()
         self._check(self.lib.ts_reset(self._ctx, _stream()))
         self.total_samples = 0
         self.num_blocks_completed = 0
@@ -269,6 +314,7 @@ class Renderer:
     # ---------------------------------------------------------------- film views
     def _film(self, which):
         import torch
+        self.flush()
         ptr = ctypes.POINTER(ctypes.c_double)()
         n = ctypes.c_size_t()
         self._check(self.lib.ts_film_buffer(self._ctx, which, ctypes.byref(ptr), ctypes.byref(n)))
@@ -313,6 +359,7 @@ class Renderer:
     def resolve_xyz(self, out=None):
         """XYZ at render resolution, [H][W][3] float32 (XYZ half of color_rays)."""
         import torch
+        self.flush()
         c = self.config
         if out is None:
             out = torch.empty((c.height, c.width, 3), dtype=torch.float32, device=self.device)
@@ -322,6 +369,7 @@ class Renderer:
 
     def resolve_xyz_host(self, out=None):
         """Same, into a (pinned) host array; the stream is synchronised."""
+        self.flush()
         c = self.config
         if out is None:
             out = np.empty((c.height, c.width, 3), np.float32)
@@ -332,6 +380,7 @@ class Renderer:
     def color_rays(self, xyz_to_rgb=None, out=None):
         """color_rays (main.py:1609-1629): [image_height][image_width][3] float32 device image."""
         import torch
+        self.flush()
         c = self.config
         if xyz_to_rgb is None:
             from .spectral_data import srgb_xyz_to_rgb
@@ -382,6 +431,7 @@ class Renderer:
     def update_materials(self, mat_f32=None, eem=None):
         """Replace the material table [M,6,B] and/or EEM table [E,B,B] (float32 CUDA tensors)."""
         import torch
+        self.flush()
         p = lambda x: None if x is None else ctypes.c_void_p(x.data_ptr())
         keep = []
         for x in (mat_f32, eem):
@@ -403,6 +453,7 @@ class Renderer:
         adj: [B,H,W] float64 CUDA tensor (dLoss / d film cell); grad: [P] float64
         CUDA tensor, P = sum(param_count()), into which the gradient is ADDED."""
         import torch
+        self.flush()
         c = self.config
         if adj.dtype != torch.float64 or tuple(adj.shape) != (c.bands, c.height, c.width) or not adj.is_contiguous():
             raise ValueError("adj must be a contiguous float64 [B, H, W] tensor")
@@ -415,6 +466,7 @@ class Renderer:
     def adjoint_passes(self, first_band, num_passes, first_pass, adj, grad):
         """adjoint_pass over num_passes consecutive passes in one launch."""
         import torch
+        self.flush()
         c = self.config
         if adj.dtype != torch.float64 or tuple(adj.shape) != (c.bands, c.height, c.width) or not adj.is_contiguous():
             raise ValueError("adj must be a contiguous float64 [B, H, W] tensor")
@@ -426,6 +478,7 @@ class Renderer:
 
     def check_device(self):
         """Raise if a kernel reported an error bit since the last check (synchronises)."""
+        self.flush()
         bits = ctypes.c_uint32()
         self._check(self.lib.ts_check_device(self._ctx, ctypes.byref(bits)))
         return bits.value

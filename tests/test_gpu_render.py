@@ -231,6 +231,37 @@ def test_render_bundles_whole_blocks(kernel, cap):
         assert torch.allclose(a, b, rtol=1e-12, atol=0)
 
 
+@pytest.mark.parametrize("kernel,cap", [("mega", 0), ("wavefront", 3 * 24 * 20)])
+def test_deferred_passes_equal_immediate(kernel, cap):
+    """defer_passes: the reference's pass-by-pass cadence, queued and launched
+    as bundles -- with a film read mid-block and a camera move mid-block, which
+    flush the queue -- renders the same films."""
+    s, c, ex, comp, bvh = setup(configs.volume_scene, width=24, height=20, medium_slices=12, medium_stacks=13,
+                                fluorescent_medium=True, depth=8)
+    B = c.bands
+    cam = s["camera"]
+    moved = np.asarray(cam["origin"], np.float64) + np.array([0.2, 0.1, -0.1])
+    out = []
+    for defer in (False, True):
+        c2 = sb.RenderConfig(**{**c.__dict__, "kernel": kernel, "queue_capacity": cap, "defer_passes": defer})
+        with sb.Renderer(s, c2, eems=ex["eems"], cmf=ex["cmf"], bvh=bvh) as r:
+            mid = None
+            for k in range(2 * B + 7):
+                r.cast_rays(k % B)
+                if k == 30:
+                    mid = r.block_film.clone()
+                if k == 40:
+                    r.update_camera(moved, cam["lookat"], cam["up"])
+                if (k + 1) % B == 0:
+                    r.average_and_reset_block((k + 1) // B)
+            out.append((r.mean_film.clone(), r.m2_film.clone(), r.block_film.clone(), mid, r.total_samples))
+            assert r.check_device() == 0
+    (a0, a1, a2, a3, t0), (b0, b1, b2, b3, t1) = out
+    assert t0 == t1 == 2 * B + 7
+    for x, y in ((a0, b0), (a1, b1), (a2, b2), (a3, b3)):
+        assert torch.allclose(x, y, rtol=1e-12, atol=0)
+
+
 def test_statistical_parity_three_sigma():
     """Independent streams: per-cell means agree within 3 combined standard errors."""
     s, c, ex, comp, bvh = setup(configs.box_scene, width=16, height=16)
