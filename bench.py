@@ -245,7 +245,8 @@ def rmse_leg(name, target, seconds, bundles=True):
     out = {"workload": name, "target": target, "blocks": nb, "spp": nb * B, "seconds": secs,
            "launch": {"kernel": best.kernel, "width": best.width, "traversal": best.traversal,
                       "block_size": best.block_size, "blocks_per_sm": best.blocks_per_sm,
-                      "occupancy": best.occupancy, "queue_capacity": best.queue_capacity},
+                      "occupancy": best.occupancy, "queue_capacity": best.queue_capacity,
+                      "trace_budget": best.trace_budget},
            "estimated_rmse": float(est), "reached": bool(est <= target),
            "launches": "one per block (wavelength bundle)" if bundles else "one per pass"}
     if est > target:
@@ -512,9 +513,11 @@ def bench_ours(args):
         tuned = {"seconds": time.time() - t0, "candidates": len(table),
                  "best": {"width": best.width, "traversal": best.traversal, "kernel": best.kernel,
                           "block_size": best.block_size, "blocks_per_sm": best.blocks_per_sm,
-                          "occupancy": best.occupancy, "queue_capacity": best.queue_capacity},
+                          "occupancy": best.occupancy, "queue_capacity": best.queue_capacity,
+                          "trace_budget": best.trace_budget},
                  "ms_per_pass": {f"w{c.width}/{c.traversal}/{c.kernel}/b{c.block_size}/s{c.blocks_per_sm}"
-                                 f"/o{c.occupancy}/q{c.queue_capacity}": round(ms, 4) for c, ms in table}}
+                                 f"/o{c.occupancy}/q{c.queue_capacity}/t{c.trace_budget}": round(ms, 4)
+                                 for c, ms in table}}
     comp = sb.compile_scene(scene, cfg.bands, eems=ex["eems"], cmf=ex["cmf"])
     bvh = sb._lib.build_bvh_host(comp.tris["v0"], comp.tris["v1"], comp.tris["v2"])
     r = sb.Renderer(scene, cfg, eems=ex["eems"], cmf=ex["cmf"], bvh=bvh, bvh_params={"width": args.width})

@@ -68,12 +68,15 @@ def default_candidates(quick=False):
 MAX_QUEUE_CAPACITY = 1 << 25
 
 
-def bundle_wavefront_candidates(npix, bands, widths=(2, 4), multiples=(2, 4, 8, 16, 32)):
+def bundle_wavefront_candidates(npix, bands, widths=(2, 4), multiples=(2, 4, 8, 16, 32), budgets=(16, 8)):
     """Regenerating-loop wavefront candidates for wavelength bundles: queue
     capacities of several frames' worth of path slots (passes in flight),
-    up to the whole bundle."""
+    up to the whole bundle, and traversal steps between lane refills (8 is
+    faster on shallow BVHs and deep volume paths, 16 on the 2.6M-triangle
+    terrain)."""
     caps = sorted({min(m * npix, bands * npix, MAX_QUEUE_CAPACITY) for m in multiples})
-    return [Candidate(w, "default", "wavefront", 256, 0, 0, 16, queue_capacity=qc) for w in widths for qc in caps]
+    return [Candidate(w, "default", "wavefront", 256, 0, 0, tb, queue_capacity=qc)
+            for w in widths for qc in caps for tb in budgets]
 
 
 def signature(compiled, cfg, bundles=False):

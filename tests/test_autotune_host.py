@@ -7,6 +7,7 @@ def test_bundle_wavefront_candidates_cover_capacities_up_to_the_bundle():
     caps = sorted({x.queue_capacity for x in c})
     assert caps == [2 << 20, 4 << 20, 8 << 20, 16 << 20, 25 << 20]
     assert {x.width for x in c} == {2, 4}
+    assert {x.trace_budget for x in c} == {8, 16} and len(c) == 2 * 5 * 2
     assert all(x.kernel == "wavefront" and x.sort_keys == 0 for x in c)
     # small frames: capped by the whole bundle; huge frames: by the slot limit
     assert max(x.queue_capacity for x in autotune.bundle_wavefront_candidates(64 * 64, 25)) == 25 * 64 * 64
