@@ -46,11 +46,45 @@ def test_create_reports_missing_device_cleanly():
     assert b"no CUDA device" in _lib.load().ts_last_error(None)
 
 
+C_SIZES = {"int32_t": 4, "uint32_t": 4, "float": 4, "double": 8, "size_t": 8, "uint64_t": 8}
+
+
+def header_struct(name):
+    """(field name, byte size) of a typedef struct of include/spectral.h, in order."""
+    src = open(os.path.join(ROOT, "include", "spectral.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    body = re.search(r"typedef struct\s*\{([^{}]*)\}\s*" + name + r"\s*;", src).group(1)
+    fields = []
+    for decl in body.split(";"):
+        decl = decl.strip()
+        if not decl:
+            continue
+        m = re.match(r"(?:const\s+)?([a-z0-9_]+)\s+(.*)", decl)
+        base, rest = m.group(1), m.group(2)
+        for item in rest.split(","):
+            item = item.strip()
+            arr = re.match(r"(\**)\s*([a-z0-9_]+)\s*(?:\[(\d+)\])?", item)
+            size = 8 if arr.group(1) else C_SIZES[base]
+            fields.append((arr.group(2), size * (int(arr.group(3)) if arr.group(3) else 1)))
+    return fields
+
+
+@pytest.mark.parametrize("cname,pytype", [("ts_config", "TsConfig"), ("ts_scene_desc", "TsSceneDesc"),
+                                          ("ts_scene_info", "TsSceneInfo"), ("ts_batch_config", "TsBatchConfig")])
+def test_ctypes_structs_match_the_header(cname, pytype):
+    """Every field of the C structs, in order and size, has its ctypes twin."""
+    from spectral_b200 import batch
+    st = getattr(_lib, pytype, None) or getattr(batch, pytype)
+    py = [(n, ctypes.sizeof(t)) for n, t in st._fields_]
+    assert py == header_struct(cname)
+
+
 def test_config_validation_on_host():
     lib = _lib.load()
     ctx = ctypes.c_void_p()
     for bad in (dict(width=0), dict(bands=0), dict(bands=65), dict(scatter_bounces=0), dict(max_path_length=-1),
-                dict(lambda_min=800.0, lambda_max=400.0)):
+                dict(lambda_min=800.0, lambda_max=400.0), dict(queue_capacity=-1), dict(queue_capacity=(1 << 25) + 1),
+                dict(occupancy=3)):
         cfg = sb.RenderConfig(**{**dict(width=4, height=4), **bad}).to_c()
         assert lib.ts_create(ctypes.byref(cfg), ctypes.byref(ctx)) == 1, bad
 
