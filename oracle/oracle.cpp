@@ -151,10 +151,19 @@ struct Rng {
   uint32_t key[2];
   uint32_t pix, scene, n = 0;
   uint32_t buf[4];
+  // function-level checks replay a given list of draws instead (0.5 past its end;
+  // the caller compares the count consumed)
+  const float *fixed = nullptr;
+  uint32_t nfixed = 0;
   Rng(uint32_t seed, uint32_t pass, uint32_t pixel, uint32_t scene_id)
       : pix(pixel), scene(scene_id) { key[0] = seed; key[1] = pass; }
   // uniform in [0, 1) with 24 random bits (exactly representable in f32)
   float next() {
+    if (fixed) {
+      const float v = n < nfixed ? fixed[n] : 0.5f;
+      ++n;
+      return v;
+    }
     if ((n & 3u) == 0) {
       const uint32_t c[4] = {pix, n >> 2, scene, 0u};
       philox_block(c, key, buf);
@@ -1226,6 +1235,116 @@ void orc_trace_brute(const orc_scene *s, const orc_config *c, const float *rays,
     }
     tri[i] = bi;
     t[i] = best;
+  }
+}
+
+// Function-level evaluation of the restated reference functions on given
+// inputs and random draws (checked against fixtures that the reference's own
+// functions computed).  Row layouts of `in` / `out` per kind are listed in
+// oracle.h.
+void orc_eval(const orc_scene *s, const orc_config *c, int32_t kind, int32_t n, const float *in, int32_t in_stride,
+              const float *draws, int32_t draw_stride, float *out, int32_t out_stride, int32_t *draws_used) {
+  const Ctx<float> x(s, c);
+  using F = float;
+  using V = V3<float>;
+  auto v3 = [](const float *p) { return V{p[0], p[1], p[2]}; };
+  auto put3 = [](float *p, V v) { p[0] = v.x; p[1] = v.y; p[2] = v.z; };
+  for (int i = 0; i < n; ++i) {
+    const float *a = in ? in + (int64_t)i * in_stride : nullptr;
+    float *o = out + (int64_t)i * out_stride;
+    Rng rng(0, 0, 0, 0);
+    rng.fixed = draws ? draws + (int64_t)i * draw_stride : nullptr;
+    rng.nfixed = draws ? (uint32_t)draw_stride : 0;
+    if (!rng.fixed) { static const float none = 0.5f; rng.fixed = &none; rng.nfixed = 0; }
+    orc_stats st{0, 0, 0, 0};
+    switch (kind) {
+      case ORC_EVAL_TRIANGLE: {  // main.py:807-829
+        const V v0 = v3(a + 6);
+        F t, u, vv;
+        hit_tri(v3(a), v3(a + 3), v0, v3(a + 9) - v0, v3(a + 12) - v0, x.eps, t, u, vv);
+        o[0] = t; o[1] = u; o[2] = vv;
+        break;
+      }
+      case ORC_EVAL_AABB:  // main.py:797-805
+        o[0] = hit_aabb(v3(a), v3(a + 3), v3(a + 6), v3(a + 9)) ? 1.f : 0.f;
+        break;
+      case ORC_EVAL_TRACE: {  // main.py:831-864
+        const Hit<F> h = trace(x, v3(a), v3(a + 3), nullptr);
+        o[0] = h.t; put3(o + 1, h.normal); put3(o + 4, h.shading_normal); o[7] = (F)h.mat;
+        o[8] = h.u; o[9] = h.v; o[10] = (F)h.is_hit; o[11] = (F)h.front; o[12] = (F)h.tri;
+        break;
+      }
+      case ORC_EVAL_COMPLEX: {  // main.py:868-896
+        const C2<F> r1 = csqrt(C2<F>{a[0], a[1]});
+        const C2<F> r2 = cdiv(C2<F>{a[0], a[1]}, C2<F>{a[2], a[3]});
+        o[0] = r1.re; o[1] = r1.im; o[2] = r2.re; o[3] = r2.im;
+        break;
+      }
+      case ORC_EVAL_FRESNEL:  // main.py:925-966
+        o[0] = fresnel<F>(a[0], a[1], a[2], a[3], a[4]);
+        break;
+      case ORC_EVAL_GGX_D:  // main.py:900-907
+        o[0] = ggx_d(x, a[0], a[1]);
+        break;
+      case ORC_EVAL_GGX_G:  // main.py:909-923
+        o[0] = ggx_g(v3(a), v3(a + 3), v3(a + 6), a[9]);
+        break;
+      case ORC_EVAL_GGX_SAMPLE:  // main.py:968-978
+        put3(o, ggx_sample(x, a[0], a[1], v3(a + 2), a[5]));
+        break;
+      case ORC_EVAL_HG:  // main.py:758-766
+        o[0] = hg_eval(x, a[0], a[1]);
+        break;
+      case ORC_EVAL_HG_SAMPLE:  // main.py:768-792
+        put3(o, hg_sample(x, v3(a), a[3], rng));
+        break;
+      case ORC_EVAL_COS_HEMISPHERE:  // main.py:689-705
+        put3(o, cosine_hemisphere(x, v3(a), rng));
+        break;
+      case ORC_EVAL_SPHERE:  // main.py:682-687
+        put3(o, random_in_unit_sphere(x, rng));
+        break;
+      case ORC_EVAL_BSDF: {  // main.py:1360-1444
+        F b, p;
+        evaluate_bsdf(x, (int)a[0], (int)a[1], v3(a + 2), v3(a + 5), v3(a + 8), (int)a[11], b, p);
+        o[0] = b; o[1] = p;
+        break;
+      }
+      case ORC_EVAL_SHADOW:  // main.py:1446-1499
+        o[0] = shadow_transmittance(x, v3(a), v3(a + 3), a[6], (int)a[7], (int)a[8], (int)a[9], &st);
+        break;
+      case ORC_EVAL_NEE: {  // main.py:1296-1358
+        Ray<F> ray{};
+        ray.pos = v3(a); ray.dir = v3(a + 3); ray.active = (int)a[6]; ray.transport = (int)a[7];
+        ray.vol = (int)a[8]; ray.thr = 1.f; ray.spdf = 1.f;
+        const Nee<F> r = sample_direct_light(x, ray, v3(a + 9), (int)a[12], rng, &st);
+        o[0] = r.factor; o[1] = r.emission; o[2] = r.weight;
+        break;
+      }
+      case ORC_EVAL_SURFACE: {  // main.py:1000-1188
+        Ray<F> ray{};
+        ray.pos = V{0.f, 0.f, 0.f}; ray.dir = v3(a); ray.active = (int)a[3]; ray.transport = (int)a[3];
+        ray.vol = (int)a[4]; ray.thr = 1.f; ray.spdf = 1.f;
+        VolEvent<F> ev{};
+        ev.hit_mat = (int)a[5]; ev.snormal = v3(a + 6); ev.normal = ev.snormal; ev.front = 1;
+        const SurfEvent<F> r = scatter_surface(x, ray, ev, rng);
+        o[0] = (F)r.did_reflect; put3(o + 1, r.dir); o[4] = r.est; o[5] = r.pdf; o[6] = (F)r.new_wl;
+        break;
+      }
+      case ORC_EVAL_VOLUME: {  // main.py:1190-1292
+        Ray<F> ray{};
+        ray.pos = v3(a); ray.dir = v3(a + 3); ray.active = (int)a[6]; ray.transport = (int)a[6];
+        ray.vol = (int)a[7]; ray.thr = 1.f; ray.spdf = 1.f; ray.pen = -1;
+        const VolEvent<F> e = scatter_volume(x, ray, rng, &st);
+        o[0] = (F)e.action; o[1] = e.travel; o[2] = e.est; put3(o + 3, e.normal); put3(o + 6, e.snormal);
+        o[9] = (F)e.front; o[10] = (F)e.hit_mat; o[11] = (F)e.tri; put3(o + 12, e.dir); o[15] = (F)e.new_wl;
+        o[16] = (F)e.pen;
+        break;
+      }
+      default:
+        break;
+    }
+    if (draws_used) draws_used[i] = (int32_t)rng.n;
   }
 }
 

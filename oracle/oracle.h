@@ -5,12 +5,19 @@
  * the package smoke check and by the CPU-baseline leg of bench.py as the
  * checker.  Nothing in the product links or calls it.
  *
- * Parity status: the reference's estimator cannot be executed here (it is
- * Taichi code and Taichi is not installable), so this restatement is pinned
- * only through the reference's own host code (golden BVH / scene / light CDF
- * / spectral data fixtures generated from it) and analytic known answers; the
- * Monte Carlo estimator itself is "parity unpinned" against Taichi's RNG and
- * fast-math codegen.
+ * Parity status: pinned to the reference's own code.  The reference's
+ * estimator is Taichi code and Taichi is not installable here, so its
+ * @ti.func functions and its cast_rays kernel were lifted unmodified out of
+ * main.py's syntax tree and run in plain Python with float32 arithmetic and
+ * given random draws (tests/golden/make_estimator_ref.py); this restatement
+ * reproduces their outputs (tests/test_oracle_pinned.py): bit for bit where
+ * the arithmetic is +, -, *, /, sqrt (intersect_triangle, intersect_aabb,
+ * trace, complex ops, GGX D and G, HG), to the last bits where it calls
+ * transcendentals, with identical branch decisions and draw counts, and per
+ * film cell to 1e-4 on whole paths of three scenes.  Host preparation (BVH,
+ * scene flattening, light CDF, spectral data) is pinned on golden fixtures
+ * the reference's host code wrote.  Not reproducible: Taichi's own random
+ * stream and its fast-math device intrinsics (last-bit differences).
  *
  * One deliberate departure: a path whose throughput is exactly zero is ended
  * (the reference keeps tracing it; its later deposits are zero, or NaN where
@@ -79,6 +86,38 @@ void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t ou
 double orc_fresnel(double cos_i, double ni, double ki, double nt, double kt, int32_t use_double);
 double orc_ggx_d(double ndh, double rough, int32_t use_double);
 double orc_hg_eval(double cos_t, double g, int32_t use_double);
+
+/* Function-level evaluation (test hook): runs one restated reference function
+ * on n rows of inputs, each with its own list of random draws (draw_stride
+ * per row; draws may be NULL), FP32.  draws_used[i] = draws row i consumed.
+ * Row layouts (in -> out):
+ *   TRIANGLE  pos3 dir3 v0_3 v1_3 v2_3            -> t u v   (intersect_triangle, main.py:807-829)
+ *   AABB      pos3 inv_dir3 min3 max3              -> hit     (intersect_aabb, main.py:797-805)
+ *   TRACE     pos3 dir3  -> t normal3 shading_normal3 mat u v is_hit front tri   (trace, main.py:831-864)
+ *   COMPLEX   z.re z.im w.re w.im                  -> sqrt(z) z/w   (main.py:868-896)
+ *   FRESNEL   cos_i ni ki nt kt                    -> R       (fresnel_spectral, main.py:925-966)
+ *   GGX_D     NdotH roughness                      -> D       (main.py:900-907)
+ *   GGX_G     n3 v3 l3 roughness                   -> G       (main.py:909-923)
+ *   GGX_SAMPLE xi0 xi1 n3 alpha                    -> h3      (main.py:968-978)
+ *   HG        cos g                                -> p       (main.py:758-766)
+ *   HG_SAMPLE dir3 g                               -> dir3    (main.py:768-792)
+ *   COS_HEMISPHERE n3                              -> dir3    (main.py:689-705)
+ *   SPHERE    (none)                               -> dir3    (main.py:682-687)
+ *   BSDF      vol surf V3 L3 N3 band               -> bsdf pdf   (evaluate_bsdf, main.py:1360-1444)
+ *   SHADOW    origin3 dir3 max_dist light_tri vol band -> T  (shadow_transmittance, main.py:1446-1499)
+ *   NEE       pos3 dir3 active transport vol N3 surf -> factor emission weight (main.py:1296-1358)
+ *   SURFACE   dir3 active vol hit_mat shading_normal3 -> did_reflect dir3 estimator pdf new_band
+ *             (scatter_surface, main.py:1000-1188; ray at the origin)
+ *   VOLUME    pos3 dir3 active vol -> action travel estimator normal3 shading_normal3 front hit_mat tri
+ *             dir3 new_band penetrated_tri   (scatter_volume, main.py:1190-1292) */
+enum {
+  ORC_EVAL_TRIANGLE = 0, ORC_EVAL_AABB = 1, ORC_EVAL_TRACE = 2, ORC_EVAL_COMPLEX = 3, ORC_EVAL_FRESNEL = 4,
+  ORC_EVAL_GGX_D = 5, ORC_EVAL_GGX_G = 6, ORC_EVAL_GGX_SAMPLE = 7, ORC_EVAL_HG = 8, ORC_EVAL_HG_SAMPLE = 9,
+  ORC_EVAL_COS_HEMISPHERE = 10, ORC_EVAL_SPHERE = 11, ORC_EVAL_BSDF = 12, ORC_EVAL_SHADOW = 13, ORC_EVAL_NEE = 14,
+  ORC_EVAL_SURFACE = 15, ORC_EVAL_VOLUME = 16
+};
+void orc_eval(const orc_scene *s, const orc_config *c, int32_t kind, int32_t n, const float *in, int32_t in_stride,
+              const float *draws, int32_t draw_stride, float *out, int32_t out_stride, int32_t *draws_used);
 
 /* Closest hit with the reference traversal (main.py:831-864): explicit stack,
  * right child popped first, no distance culling.  rays: [n][6] (pos, dir).

@@ -74,6 +74,8 @@ def lib():
         L.orc_build_bvh_sweep.argtypes = [ctypes.c_int32, F32P, F32P, F32P, ctypes.c_int32, F32P, F32P,
                                           I32P, I32P, I32P, I32P, I32P]
         L.orc_build_bvh_sweep.restype = ctypes.c_int32
+        L.orc_eval.argtypes = [ctypes.POINTER(OrcScene), ctypes.POINTER(OrcConfig), ctypes.c_int32, ctypes.c_int32,
+                               F32P, ctypes.c_int32, F32P, ctypes.c_int32, F32P, ctypes.c_int32, I32P]
         d = ctypes.c_double
         L.orc_fresnel.argtypes = [d, d, d, d, d, ctypes.c_int32]
         L.orc_fresnel.restype = d
@@ -150,6 +152,31 @@ class Scene:
             v = np.asarray(arrays[k], dtype=np.float32)
             setattr(s, k, (ctypes.c_float * 3)(*v.tolist()))
         self.s = s
+
+
+# function-level hooks of orc_eval: kind -> (id, output width)
+EVAL_KINDS = {"triangle": (0, 3), "aabb": (1, 1), "trace": (2, 13), "complex": (3, 4), "fresnel": (4, 1),
+              "ggx_d": (5, 1), "ggx_g": (6, 1), "ggx_sample": (7, 3), "hg": (8, 1), "hg_sample": (9, 3),
+              "cos_hemisphere": (10, 3), "sphere": (11, 3), "bsdf": (12, 2), "shadow": (13, 1), "nee": (14, 3),
+              "surface": (15, 7), "volume": (16, 17)}
+
+
+def eval_fn(kind, cfg, inputs=None, draws=None, scene=None, n=None):
+    """Run one restated reference function (FP32) on rows of inputs, each row
+    with its own list of random draws.  Returns (outputs [n, w], draws used [n])."""
+    k, width = EVAL_KINDS[kind]
+    inp = None if inputs is None else _f32(inputs)
+    if inp is not None and inp.ndim == 1:
+        inp = inp[:, None]
+    dr = None if draws is None else _f32(draws)
+    n = n if n is not None else (inp.shape[0] if inp is not None else dr.shape[0])
+    out = np.zeros((n, width), np.float32)
+    used = np.zeros(n, np.int32)
+    lib().orc_eval(ctypes.byref(scene.s) if scene is not None else None, ctypes.byref(cfg.c), k, n,
+                   None if inp is None else _p(inp, F32P), 0 if inp is None else inp.shape[1],
+                   None if dr is None else _p(dr, F32P), 0 if dr is None else dr.shape[1], _p(out, F32P), width,
+                   _p(used, I32P))
+    return out, used
 
 
 def fresnel(cos_i, ni, ki, nt, kt, use_double=False):

@@ -27,11 +27,17 @@ def pytest_collection_modifyitems(config, items):
             it.add_marker(skip)
 
 
-REFERENCE_TREE = "/root/reference"
+def reference_dir():
+    """Location of a reference checkout: $SPECTRAL_REFERENCE_DIR, else a
+    checkout named ``reference`` beside this repository (None if absent)."""
+    d = os.environ.get("SPECTRAL_REFERENCE_DIR") or os.path.join(
+        os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))), "reference")
+    return d if os.path.isfile(os.path.join(d, "main.py")) else None
 
 
 @pytest.fixture
 def reference_tree():
-    if not os.path.isdir(REFERENCE_TREE):
-        pytest.skip("reference checkout not present")
-    return REFERENCE_TREE
+    d = reference_dir()
+    if d is None:
+        pytest.skip("reference checkout not present (set SPECTRAL_REFERENCE_DIR)")
+    return d

@@ -2,7 +2,8 @@
 
 Run once, in a container where the reference checkout is present:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <reference checkout>
+    (or set SPECTRAL_REFERENCE_DIR)
 
 What is pinned (each array is produced by the reference's own code, unmodified):
 
@@ -170,4 +171,7 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SPECTRAL_REFERENCE_DIR")
+    if not ref or not os.path.isfile(os.path.join(ref, "main.py")):
+        sys.exit("usage: make_golden.py <reference checkout> (or set SPECTRAL_REFERENCE_DIR)")
+    main(ref)
