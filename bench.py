@@ -1,17 +1,21 @@
-"""Benchmark: spectral path-tracing sample passes on the large-mesh workload.
+"""Benchmark: spectral path tracing on the large-mesh workload.
 
-One step = one sample pass (cast_rays) over every pixel of the workload at
-one wavelength band: 1024x1024 paths of depth <= 12 through a 2.59M-triangle
-scene (1024^2-vertex heightfield + 500k-triangle displaced sphere, GGX
-conductors, 8 emissive quads, 25 bands over 380-740 nm).  The metric is
-Mpaths/s (one path = one pixel x one band-pass, the reference's unit).
+One step = one spectral block: the 25 sample passes of a wavelength cycle
+(cast_rays at bands 0..24, each pass its own random stream) over every pixel
+of the workload -- 1024x1024 paths per pass of depth <= 12 through a
+2.59M-triangle scene (1024^2-vertex heightfield + 500k-triangle displaced
+sphere, GGX conductors, 8 emissive quads, 25 bands over 380-740 nm).  The
+metric is Mpaths/s (one path = one pixel x one band-pass, the reference's
+unit); a step is 26.2M paths.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
-                  [--kernel mega|wavefront] [--workload terrain|box|volume]
+                  [--kernel mega|wavefront] [--workload terrain|box|volume|batch|adjoint|rmse]
 
 --impl reference times the reference's CPU path: the FP32 restatement of its
-estimator (oracle/, OpenMP over all host threads), since the reference's own
-Taichi kernels cannot be installed here.
+estimator (oracle/, pinned to the reference's own code; OpenMP over all host
+threads) on the reference's BVH algorithm (the oracle's full-sweep SAH
+builder), since the reference's own Taichi kernels cannot be installed here.
+That arm loads no part of the CUDA library.
 """
 import argparse
 import json
@@ -36,8 +40,8 @@ BYTES_DEPOSIT = 16   # FP64 read-modify-write of a film cell
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=300)
-    p.add_argument("--warmup", type=int, default=10)
+    p.add_argument("--steps", type=int, default=20, help="timed steps (spectral blocks of 25 passes)")
+    p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--kernel", default="mega", choices=["mega", "wavefront"])
     p.add_argument("--workload", default="terrain", choices=["terrain", "box", "volume", "batch", "adjoint"])
@@ -45,7 +49,7 @@ def parse():
     p.add_argument("--traversal", default="default", choices=["default", "speculative"])
     p.add_argument("--occupancy", type=int, default=0, choices=[0, 8], help="megakernel register budget (--no-tune)")
     p.add_argument("--launch", default="bundle", choices=["bundle", "pass"],
-                   help="render the timed passes 25 per launch (wavelength bundles) or one per launch")
+                   help="render each step's 25 passes in one launch (a wavelength bundle) or one launch per pass")
     p.add_argument("--budget", type=int, default=0, help="wavefront traversal steps between refills")
     p.add_argument("--queue-capacity", type=int, default=0,
                    help="wavefront path slots of the regenerating loop (--no-tune; 0 = one per pixel)")
@@ -76,6 +80,30 @@ def workload(name):
         desc = ("volume: box + 20k-tri HG medium (g 0.7) + fluorescent wall; 512x512, depth 32, 25 bands, "
                 "512 spp")
     return scene, cfg, ex, desc
+
+
+def step_config(cfg, ex, desc, world, num_tris):
+    """The workload as both arms report it (identical dictionaries)."""
+    npix = cfg.width * cfg.height
+    # resident inputs: 96 B per triangle (positions + shading normals) and the
+    # three FP64 film planes (block, mean, second moment)
+    mb = (96 * num_tris + 3 * 8 * cfg.bands * npix) / 1e6
+    l2 = ("inputs larger than L2: %.0f MB of triangles and film > 126 MB L2; no flush" % mb if mb > 126 else
+          "inputs fit in L2 (%.0f MB of triangles and film): steady-state rate of a resident scene, no flush" % mb)
+    return {"workload": desc, "paths_per_step": cfg.bands * npix, "passes_per_step": cfg.bands,
+            "pixels": npix, "spp": ex["spp"], "passes_for_spp": cfg.samples_per_pixel, "l2": l2,
+            "parallelism": f"{world} GPU(s), disjoint sample passes per GPU"}
+
+
+def reference_tree(comp):
+    """The reference's BVH algorithm (main.py:437-507: full-sweep SAH, <= 10
+    triangles per leaf) restated in the oracle, in the reference layout."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import orc
+    t = comp.tris
+    b = orc.build_bvh_sweep(t["v0"], t["v1"], t["v2"])
+    b["tri_perm"] = b.pop("perm")
+    return b
 
 
 def dist_env():
@@ -433,45 +461,58 @@ def bench_batch(args):
 
 
 def bench_reference(args):
-    """CPU arm: the reference estimator (oracle restatement) on all host threads."""
+    """CPU arm: the reference's estimator (the oracle restatement, pinned to the
+    reference's own code) on all host threads, traversing the reference's BVH
+    algorithm in the reference's order without distance culling.  Loads no
+    part of the CUDA library: the scene comes from the workload generator and
+    the host-side flattening (pure Python), the tree from the oracle.  Each
+    step renders a random pixel sample of every pass of one spectral block
+    (the same 25 band-passes as a GPU step), sized so that the run ends in a
+    few minutes."""
     import numpy as np
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    import spectral_b200 as sb
+    from spectral_b200 import scene as sbscene
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import orc
     scene, cfg, ex, desc = workload(args.workload)
-    comp = sb.compile_scene(scene, cfg.bands, eems=ex["eems"], cmf=ex["cmf"])
-    bvh = sb._lib.build_bvh_host(comp.tris["v0"], comp.tris["v1"], comp.tris["v2"])
+    comp = sbscene.compile_scene(scene, cfg.bands, eems=ex["eems"], cmf=ex["cmf"])
+    t0 = time.perf_counter()
+    bvh = reference_tree(comp)
+    tree_s = time.perf_counter() - t0
     osc = orc.oracle_scene(comp, bvh, scene["camera"])
     ocfg = orc.oracle_config(cfg)
+    B = cfg.bands
     npix = cfg.width * cfg.height
     rng = np.random.default_rng(7)
-    # size each step so that the whole run takes ~2 minutes
     pix = rng.choice(npix, 1024, replace=False).astype(np.int32)
     t = time.perf_counter()
     orc.render_pass(osc, ocfg, 0, 0, pix)
     rate = 1024 / max(time.perf_counter() - t, 1e-6)
-    per_step = int(min(npix, max(256, rate * min(0.5, 120.0 / max(1, args.steps + args.warmup)))))
+    # pixels per pass of a step: ~150 s for the whole run, at most 2 s a step
+    per_pass = int(min(npix, max(64, rate * min(2.0, 150.0 / max(1, args.steps + args.warmup)) / B)))
+
+    def step(k):
+        for b in range(B):
+            px = rng.choice(npix, per_pass, replace=False).astype(np.int32)
+            orc.render_pass(osc, ocfg, k * B + b, b, px)
+
     for w in range(args.warmup):
-        pix = rng.choice(npix, per_step, replace=False).astype(np.int32)
-        orc.render_pass(osc, ocfg, w, w % cfg.bands, pix)
-    total = 0.0
+        step(w)
+    t = time.perf_counter()
     for k in range(args.steps):
-        pix = rng.choice(npix, per_step, replace=False).astype(np.int32)
-        t = time.perf_counter()
-        orc.render_pass(osc, ocfg, args.warmup + k, k % cfg.bands, pix)
-        total += time.perf_counter() - t
-    mpaths = per_step * args.steps / total / 1e6
+        step(args.warmup + k)
+    total = time.perf_counter() - t
+    mpaths = per_pass * B * args.steps / total / 1e6
     threads = os.cpu_count() or 1
-    sample = f"{per_step} random pixels of one band-pass per step (of {npix} per full pass)"
+    sample = (f"{per_pass} random pixels of each of the {B} band-passes of a step (of {npix} per pass); "
+              f"reference BVH algorithm (full-sweep SAH, built in {tree_s:.1f} s), reference traversal order")
     line = {"impl": "reference", "metric": "Mpaths/s", "value": mpaths, "unit": "Mpaths/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded procedural scene)",
-            "config": {"workload": desc, "paths_per_step": per_step, "bvh": "library binned-SAH tree in the "
-                       "reference layout, traversed in the reference order without distance culling"},
+            "data": "synthetic (seeded procedural scene; no dataset)",
+            "config": step_config(cfg, ex, desc, world, comp.num_tris),
             "cpu_baseline": {"value": mpaths, "unit": "Mpaths/s", "cores": threads, "kind": "port",
                              "sample": sample},
             "e2e": {"value": mpaths, "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -522,19 +563,31 @@ def bench_ours(args):
     bvh = sb._lib.build_bvh_host(comp.tris["v0"], comp.tris["v1"], comp.tris["v2"])
     r = sb.Renderer(scene, cfg, eems=ex["eems"], cmf=ex["cmf"], bvh=bvh, bvh_params={"width": args.width})
     B = cfg.bands
-    paths_per_step = cfg.width * cfg.height
-    base_pass = rank * (args.warmup + args.steps + 8) * 4  # disjoint random streams per rank
+    npix = cfg.width * cfg.height
+    paths_per_step = B * npix  # one step = one spectral block of B passes
+    base_pass = rank * (args.warmup + args.steps + 64) * B * 4  # disjoint random streams per rank
+    use_bundles = args.launch == "bundle" and (args.kernel == "mega" or cfg.sort_keys == 0)
+    wave_loop = args.kernel == "wavefront" and (use_bundles or cfg.queue_capacity > 0) and cfg.sort_keys == 0
+
+    def step(k, first_pass):
+        """Step k: the B passes of one spectral block (bands 0..B-1)."""
+        p0 = first_pass + k * B
+        if use_bundles:
+            r.cast_rays_bundle(0, B, pass_idx=p0)
+        else:
+            for b in range(B):
+                r.cast_rays(b, pass_idx=p0 + b)
 
     # warm-up, then one counted pass (work counters for the roofline's algorithmic bytes)
     for w in range(args.warmup):
-        r.cast_rays(w % B, pass_idx=base_pass + w)
-    work = r.cast_rays_counted(12, pass_idx=base_pass + args.warmup)
+        step(w, base_pass)
+    work = r.cast_rays_counted(12, pass_idx=base_pass + 1)
     torch.cuda.synchronize()
     node_bytes = BYTES_NODE * (args.width // 2)  # 2 -> 64 B, 4 -> 128 B, 8 -> 256 B
     bytes_per_path = (node_bytes * work["node_visits"] + BYTES_TRI * work["tri_tests"] + BYTES_HIT * work["hits"]
                       + BYTES_MAT_VERTEX * work["vertices"] + BYTES_DEPOSIT * work["deposits"]) / work["paths"]
 
-    # ---- timed region: K passes, device time, max over ranks
+    # ---- timed region: K steps, device time, max over ranks
     sampler = ClockSampler(gpu_uuid(local))
     if world > 1:
         dist.barrier()
@@ -542,19 +595,10 @@ def bench_ours(args):
     sampler.start()
     time.sleep(0.3)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    # wavelength bundles: the megakernel, or the wavefront's regenerating loop (unsorted queues)
-    use_bundles = args.launch == "bundle" and (args.kernel == "mega" or cfg.sort_keys == 0)
-    wave_loop = args.kernel == "wavefront" and (use_bundles or cfg.queue_capacity > 0) and cfg.sort_keys == 0
+    timed_first = base_pass + (args.warmup + 1) * B
     e0.record()
-    k = 0
-    while k < args.steps:  # exactly K passes; whole wavelength bundles when asked, single passes after
-        p0 = base_pass + args.warmup + 1 + k
-        if use_bundles and args.steps - k >= B:
-            r.cast_rays_bundle(k % B, B, pass_idx=p0)
-            k += B
-        else:
-            r.cast_rays(k % B, pass_idx=p0)
-            k += 1
+    for k in range(args.steps):
+        step(k, timed_first)
     e1.record()
     torch.cuda.synchronize()
     clocks = sampler.stop()
@@ -568,7 +612,30 @@ def bench_ours(args):
     value = world * args.steps * paths_per_step / (ms_max * 1e-3) / 1e6
     bits = r.check_device()
 
-    loop_iters = r.wave_loop_iterations() if wave_loop else 0  # of the last timed launch
+    # ---- kernels launched in the timed region: the same steps again, untimed
+    # (the same passes, so the same paths), reading each loop launch's iterations
+    if wave_loop:
+        iters = []
+        for k in range(args.steps):
+            if use_bundles:
+                step(k, timed_first)
+                iters.append(r.wave_loop_iterations())
+            else:
+                for b in range(B):
+                    r.cast_rays(b, pass_idx=timed_first + k * B + b)
+                    iters.append(r.wave_loop_iterations())
+        # a loop launch: the init kernel, then trace + shade + control per iteration
+        gpu_launches = sum(1 + 3 * it for it in iters)
+        launches = ("one regenerating wavefront loop per %s (init kernel, then a CUDA-graph while-loop of trace, "
+                    "shade, control; %.1f iterations per launch)" % ("step (25-pass bundle)" if use_bundles
+                                                                     else "pass", sum(iters) / len(iters)))
+    elif args.kernel == "mega":
+        gpu_launches = args.steps * (1 if use_bundles else B)
+        launches = "one megakernel launch per " + ("step (25-pass bundle)" if use_bundles else "pass")
+    else:
+        gpu_launches = args.steps * B * (2 + 2 * cfg.max_path_length)
+        launches = "depth-synchronous wavefront: generate, then trace + shade per depth, per pass"
+    torch.cuda.synchronize()
 
     # ---- end to end through the public API with host buffers, at the
     # reference's cadence (main.py:1826-1837): per step the camera in, one
@@ -576,19 +643,14 @@ def bench_ours(args):
     # (average_and_reset_block) and the resolved XYZ image out (pinned)
     out = torch.empty((cfg.height, cfg.width, 3), dtype=torch.float32, pin_memory=True).numpy()
     cam = scene["camera"]
-    e2e_blocks = max(4, args.steps // B // 2)
     r.clear_pixel_space()
     torch.cuda.synchronize()
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2e_first = base_pass + (args.warmup + args.steps + 8) * B
     f0.record()
-    for k in range(e2e_blocks):
+    for k in range(args.steps):
         r.update_camera(cam["origin"], cam["lookat"], cam["up"])
-        p0 = base_pass + 7 * (args.steps + 1) + k * B
-        if use_bundles:
-            r.cast_rays_bundle(0, B, pass_idx=p0)
-        else:
-            for b in range(B):
-                r.cast_rays(b, pass_idx=p0 + b)
+        step(k, e2e_first)
         r.average_and_reset_block(k + 1)
         r.resolve_xyz_host(out)
     f1.record()
@@ -597,84 +659,72 @@ def bench_ours(args):
     t2 = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(t2, op=dist.ReduceOp.MAX)
-    e2e_value = world * e2e_blocks * B * paths_per_step / (float(t2.item()) * 1e-3) / 1e6
+    e2e_value = world * args.steps * paths_per_step / (float(t2.item()) * 1e-3) / 1e6
 
-    launches_per_step = 1 if args.kernel == "mega" else 2 + 2 * cfg.max_path_length
-    if use_bundles:
-        # a bundle: one megakernel launch, or the loop's init kernel plus three kernels per iteration
-        launches_per_step = (1.0 + 3 * loop_iters if wave_loop else 1.0) / B
     peak, peak_src = measured_peak()
     step_s = ms_max * 1e-3 / args.steps
     achieved = bytes_per_path * paths_per_step / step_s / 1e9
     traffic = profiled_traffic(args.kernel, args.workload, args.width, 0 if wave_loop else args.occupancy,
                                use_bundles)
+    kernel_name = ("k_render_mega" if args.kernel == "mega" else
+                   "regenerating wavefront loop (k_trace + k_shade_loop + k_loop_control per iteration)"
+                   if wave_loop else "depth-synchronous wavefront pass")
 
     line = {"metric": "Mpaths/s", "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded procedural scene; no dataset)",
-            "config": {"workload": desc, "kernel": args.kernel, "bvh_width": args.width, "traversal": args.traversal,
+            "config": step_config(cfg, ex, desc, world, comp.num_tris),
+            "launch": {"kernel": args.kernel, "bvh_width": args.width, "traversal": args.traversal,
                        "occupancy": args.occupancy, "queue_capacity": cfg.queue_capacity,
-                       "launches": (("one regenerating wavefront loop per 25-pass wavelength bundle (init kernel, "
-                                     "then a CUDA-graph while-loop of trace, shade, control; %d iterations)"
-                                     % loop_iters if wave_loop else
-                                     "one launch per 25-pass wavelength bundle") +
-                                    " (each pass its own band, the same paths as one launch per pass)"
-                                    if use_bundles else "one launch per pass"),
-                       "paths_per_step": paths_per_step,
-                       "spp": ex["spp"], "passes_for_spp": cfg.samples_per_pixel,
-                       "l2": "inputs larger than L2: scene %.0f MB + film %.0f MB > 126 MB L2; no flush"
-                             % ((r.scene_info()["device_bytes"] - 3 * paths_per_step * B * 8) / 1e6,
-                                paths_per_step * B * 8 / 1e6),
-                       "parallelism": f"{world} GPU(s), disjoint sample passes per GPU"},
+                       "block_size": cfg.block_size, "trace_budget": cfg.trace_budget, "launches": launches},
             "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": 36,
-                    "d2h_bytes_per_step": int(out.nbytes), "passes_per_step": B,
+                    "d2h_bytes_per_step": int(out.nbytes),
                     "what": "per step (one spectral block): Renderer.update_camera + %s + "
                             "average_and_reset_block + resolve_xyz_host (pinned host XYZ image), through the C ABI"
                             % ("cast_rays_bundle of the block's %d passes" % B if use_bundles
                                else "%d cast_rays" % B)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "traffic_per": "pass (ncu capture of a launch of the same configuration, per pass)",
-                         "kernel": ("k_render_mega" if args.kernel == "mega" else
-                                    "wavefront loop (k_trace + k_shade_loop + k_loop_control per iteration)"
-                                    if wave_loop else "wavefront pass"),
-                         "bytes_per_path": bytes_per_path, "peak_source": peak_src,
+                         "frac": achieved / peak,
+                         "traffic": None if traffic is None else traffic * B,
+                         "traffic_per": "step (one launch of the timed configuration: DRAM bytes per pass from an "
+                                        "ncu capture x 25 passes)",
+                         "kernel": kernel_name, "bytes_per_path": bytes_per_path,
+                         "bytes_per_launch": bytes_per_path * paths_per_step, "peak_source": peak_src,
                          "work_per_path": {k: v / work["paths"] for k, v in work.items() if k != "paths"}},
-            "gpu_launches": int(round(launches_per_step * args.steps + (args.steps % B if use_bundles else 0))),
+            "gpu_launches": int(gpu_launches),
             "autotune": tuned,
             "clocks": clocks, "device_error_bits": bits}
 
     line["vertices_per_s"] = value * 1e6 * work["vertices"] / work["paths"]
-    if use_bundles:
-        # the same passes with one launch per pass (the reference's cadence), for comparison
-        torch.cuda.synchronize()
-        h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        n1 = 2 * B
-        h0.record()
-        for k in range(n1):
-            r.cast_rays(k % B, pass_idx=base_pass + 8000 + k)
-        h1.record()
-        torch.cuda.synchronize()
-        line["one_launch_per_pass"] = {"value": paths_per_step / (h0.elapsed_time(h1) / n1 * 1e-3) / 1e6,
-                                       "unit": "Mpaths/s", "ms_per_pass": h0.elapsed_time(h1) / n1}
+    # the same passes with one launch per pass (the reference's cadence), for comparison
+    torch.cuda.synchronize()
+    h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n1 = 2 * B
+    h0.record()
+    for k in range(n1):
+        r.cast_rays(k % B, pass_idx=base_pass + 40000 + k)
+    h1.record()
+    torch.cuda.synchronize()
+    line["one_launch_per_pass"] = {"value": npix / (h0.elapsed_time(h1) / n1 * 1e-3) / 1e6,
+                                   "unit": "Mpaths/s", "ms_per_pass": h0.elapsed_time(h1) / n1}
     if rank == 0 and world == 1 and not args.no_extras:
         # the plain single-scene wavefront kernel on the same workload (same paths)
         r.set_launch_config(kernel="wavefront", traversal="default", block_size=128, blocks_per_sm=0, sort_keys=0,
                             trace_budget=16, occupancy=0, queue_capacity=0)
         for k in range(3):
-            r.cast_rays(k % B, pass_idx=base_pass + 9000 + k)
+            r.cast_rays(k % B, pass_idx=base_pass + 41000 + k)
         torch.cuda.synchronize()
         g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        nw = max(10, args.steps // 10)
+        nw = 2 * B
         g0.record()
         for k in range(nw):
-            r.cast_rays(k % B, pass_idx=base_pass + 9100 + k)
+            r.cast_rays(k % B, pass_idx=base_pass + 41100 + k)
         g1.record()
         torch.cuda.synchronize()
         wms = g0.elapsed_time(g1) / nw
-        line["plain_wavefront"] = {"value": paths_per_step / (wms * 1e-3) / 1e6, "unit": "Mpaths/s",
-                                   "ms_per_step": wms, "bvh_width": args.width, "trace_budget": 16}
+        line["plain_wavefront"] = {"value": npix / (wms * 1e-3) / 1e6, "unit": "Mpaths/s",
+                                   "ms_per_pass": wms, "bvh_width": args.width, "trace_budget": 16}
     if rank == 0 and world == 1 and not args.no_extras:
         line["rmse"] = [rmse_leg("box", 0.01, args.rmse_seconds, bundles=True),
                         rmse_leg("box", 0.01, args.rmse_seconds, bundles=False),
@@ -682,10 +732,11 @@ def bench_ours(args):
                         rmse_leg("volume", 0.05, args.rmse_seconds, bundles=True)]
         line["adjoint"] = adjoint_leg()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, n, dt, threads, st = cpu_oracle_rate(comp, bvh, scene, cfg, seconds=12.0)
+        rate, n, dt, threads, st = cpu_oracle_rate(comp, reference_tree(comp), scene, cfg, seconds=12.0)
         line["cpu_baseline"] = {"value": rate / 1e6, "unit": "Mpaths/s", "cores": threads, "kind": "port",
-                                "sample": f"{n} paths of the workload's band-passes ({dt:.1f} s, FP32 oracle, "
-                                          f"reference traversal order)"}
+                                "sample": f"{n} paths of the workload's band-passes ({dt:.1f} s, FP32 oracle "
+                                          f"pinned to the reference's code, reference BVH algorithm and "
+                                          f"traversal order)"}
     r.close()
     if world > 1:
         dist.destroy_process_group()

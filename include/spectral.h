@@ -159,6 +159,16 @@ ts_status ts_render_passes(ts_ctx *ctx, uint32_t first_pass, int32_t num_passes,
  * one shade and one control kernel); synchronises the stream.  0 before any. */
 ts_status ts_wave_loop_iterations(ts_ctx *ctx, void *stream, int32_t *iterations);
 
+/* Bound on the iterations of one regenerating-loop launch (new; the reference
+ * has no device-side loop).  0 (the default) = the automatic bound, which no
+ * launch reaches unless its queues are corrupt: every slot starts a new work
+ * item at least once per max_path_length iterations while items are left.  A
+ * smaller positive limit applies when tighter.  A launch that reaches the
+ * bound stops on the device (its remaining paths are dropped) and sets the
+ * iteration-cap bit that ts_check_device reports as TS_ERR_DEVICE_FAULT; the
+ * next launch starts clean.  For failure-handling tests and watchdogs. */
+ts_status ts_set_loop_iteration_limit(ts_ctx *ctx, int32_t limit);
+
 /* The same pass rendered by the plain megakernel with work counters (used to
  * derive algorithmic bytes per path).  work[0..6] = paths, path vertices,
  * traversals, BVH node visits, triangle tests, hits resolved, film deposits;
@@ -176,10 +186,13 @@ ts_status ts_render_pass_counted(ts_ctx *ctx, uint32_t pass_idx, int32_t band, v
  * camera, with the same random streams as ts_render_pass, ADDING deposits into
  * film_dev: a caller-owned [B][H][W] float64 device buffer of the frame.
  * At most 65536 pixels per call (TS_ERR_CAPACITY beyond).  Its scratch is a
- * static device array of about 8.4 MB that every GPU loading the library keeps
- * until exit; the first call on a device looks its address up, so make that
- * first call before any stream capture.  All calls share the array: calls that
- * overlap on the GPU race and must be serialised by the caller. */
+ * static device array of about 8.4 MB that every GPU using it keeps until
+ * exit.  The CUDA runtime loads it lazily: the first call on a device (or an
+ * earlier wavefront launch of this library there) reserves the array and
+ * looks its address up, so a host with a fixed memory budget makes that first
+ * call during start-up, before any stream capture.  The address is looked up
+ * again in a new context (after a device reset).  All calls share the array:
+ * calls that overlap on the GPU race and must be serialised by the caller. */
 ts_status ts_render_tile_noalloc(ts_ctx *ctx, uint32_t pass_idx, int32_t band, int32_t x0, int32_t y0,
                                  int32_t tile_w, int32_t tile_h, double *film_dev, void *stream);
 

@@ -47,6 +47,7 @@ struct ts_ctx {
   ts::WaveBuffers wave{};
   std::vector<void *> wave_allocs;
   ts::WaveLoopGraph *wave_loop = nullptr;  // captured regenerating wavefront loop
+  int loop_limit = 0;                      // caller's bound on loop iterations per launch (0 = automatic)
   size_t film_bytes = 0, scene_bytes = 0, wave_bytes = 0;
   float cam[9] = {0, 0, 3.5f, 0, 0, -1, 0, 1, 0};
   std::string err;
@@ -501,7 +502,7 @@ static ts_status render_wave_loop(ts_ctx *c, uint32_t pass0, int npass, int band
   if (per_sm <= 0) per_sm = std::max(1, 2048 / bs);
   TS_CUDA(c, ts::launch_wave_loop(c->ds, c->dc, pass0, band0, npass, film_of(c), c->wave, c->d_err,
                                   c->num_sms * per_sm, bs, st, c->cfg.trace_budget, cap, &c->wave_loop,
-                                  c->cfg.loop_host != 0),
+                                  c->cfg.loop_host != 0, c->loop_limit),
           what);
   return TS_OK;
 }
@@ -564,6 +565,13 @@ ts_status ts_render_passes(ts_ctx *c, uint32_t first_pass, int32_t num_passes, i
   TS_CUDA(c, ts::launch_render_mega(c->ds, c->dc, first_pass, first_band, film_of(c), c->d_counter, c->d_err,
                                     c->num_sms * per_sm, bs, as_stream(stream), nullptr, num_passes, c->cfg.occupancy),
           "ts_render_passes");
+  return TS_OK;
+}
+
+ts_status ts_set_loop_iteration_limit(ts_ctx *c, int32_t limit) {
+  if (!c) return fail(nullptr, TS_ERR_INVALID_ARG, "ts_set_loop_iteration_limit: null context");
+  if (limit < 0) return fail(c, TS_ERR_INVALID_ARG, "ts_set_loop_iteration_limit: limit must be >= 0");
+  c->loop_limit = limit;
   return TS_OK;
 }
 

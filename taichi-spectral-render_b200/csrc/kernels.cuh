@@ -85,7 +85,8 @@ struct WaveLoopGraph;
 // host_driven: launch the iterations from the host instead (one stream sync each)
 cudaError_t launch_wave_loop(const DevScene &s, const DevConfig &c, uint32_t pass0, int band0, int npass, Film f,
                              const WaveBuffers &w, uint32_t *err, int grid, int block, cudaStream_t st,
-                             int trace_budget, int capacity, WaveLoopGraph **graph, bool host_driven = false);
+                             int trace_budget, int capacity, WaveLoopGraph **graph, bool host_driven = false,
+                             int limit_override = 0);
 void free_wave_loop(WaveLoopGraph *graph);
 
 // ---- path-replay adjoint (adjoint.cu) -----------------------------------------

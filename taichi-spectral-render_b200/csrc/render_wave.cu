@@ -350,8 +350,15 @@ __device__ __forceinline__ void shade_path(const DevScene &s, const DevConfig &c
   }
 }
 
-__device__ __forceinline__ void append_shadow(int *count, const WaveBuffers &w, const Shaded &r) {
+// Queue appends are bounded by construction (every slot appends at most once
+// per stage); the checks below only keep a corrupted counter from writing
+// past a queue, reporting kErrQueueOverflow instead.
+__device__ __forceinline__ void append_shadow(int *count, const WaveBuffers &w, const Shaded &r, uint32_t *err) {
   const int sslot = warp_append(count, r.nee);
+  if (r.nee && sslot >= w.capacity) {
+    atomicOr(err, kErrQueueOverflow);
+    return;
+  }
   if (r.nee) {
     w.sq_origin[sslot] = make_float4(r.sq.origin.x, r.sq.origin.y, r.sq.origin.z, r.sq.max_dist);
     w.sq_dir[sslot] = make_float4(r.sq.dir.x, r.sq.dir.y, r.sq.dir.z, r.sq.contrib);
@@ -359,8 +366,15 @@ __device__ __forceinline__ void append_shadow(int *count, const WaveBuffers &w, 
   }
 }
 
+__device__ __forceinline__ void append_ext(int *count, int *q, int pid, bool want, int capacity, uint32_t *err) {
+  const int slot = warp_append(count, want);
+  if (!want) return;
+  if (slot < capacity) q[slot] = pid;
+  else atomicOr(err, kErrQueueOverflow);
+}
+
 __global__ void __launch_bounds__(kMaxBlock) k_shade(DevScene s, DevConfig c, uint32_t pass, int band, int depth,
-                                               Film f, WaveBuffers w, int use_sorted) {
+                                               Film f, WaveBuffers w, int use_sorted, uint32_t *err) {
   const int n = w.counts[kCntExt + depth];
   const int *q = use_sorted ? w.sorted : w.queue[depth & 1];
   int *qn = w.queue[(depth + 1) & 1];
@@ -379,9 +393,8 @@ __global__ void __launch_bounds__(kMaxBlock) k_shade(DevScene s, DevConfig c, ui
       pid = q[i];
       shade_path(s, c, pass, band, last, f, w, pid, false, r);
     }
-    append_shadow(w.counts + kCntSh + depth, w, r);
-    const int qslot = warp_append(w.counts + kCntExt + depth + 1, r.cont);
-    if (r.cont) qn[qslot] = pid;
+    append_shadow(w.counts + kCntSh + depth, w, r, err);
+    append_ext(w.counts + kCntExt + depth + 1, qn, pid, r.cont, w.capacity, err);
   }
 }
 
@@ -432,7 +445,8 @@ __global__ void k_loop_init(DevScene s, DevConfig c, WaveBuffers w, WaveLoop *L,
 
 // 64 registers (4 resident 256-thread blocks per SM; a few spills): faster
 // than the unbounded 111-register build by 4-6 % on whole-bundle loops
-__global__ void __launch_bounds__(kMaxBlock, 4) k_shade_loop(DevScene s, DevConfig c, Film f, WaveBuffers w, WaveLoop *L) {
+__global__ void __launch_bounds__(kMaxBlock, 4) k_shade_loop(DevScene s, DevConfig c, Film f, WaveBuffers w, WaveLoop *L,
+                                                          uint32_t *err) {
   const int a = L->iter & 1;
   const int n = L->ext[a];
   const int *q = w.queue[a];
@@ -462,7 +476,7 @@ __global__ void __launch_bounds__(kMaxBlock, 4) k_shade_loop(DevScene s, DevConf
       shade_path(s, c, pass0 + (uint32_t)po, band, (tag & 0xffff) + 1 >= c.max_depth, f, w, pid, shared, r);
       if (r.cont) w.tag[pid] = tag + 1;
     }
-    append_shadow(L->sh + a, w, r);
+    append_shadow(L->sh + a, w, r, err);
     // the slots of ended paths start the next work items
     bool fresh = false;
     if (more) {
@@ -476,8 +490,7 @@ __global__ void __launch_bounds__(kMaxBlock, 4) k_shade_loop(DevScene s, DevConf
         fresh = true;
       }
     }
-    const int qslot = warp_append(L->ext + (a ^ 1), r.cont || fresh);
-    if (r.cont || fresh) qn[qslot] = pid;
+    append_ext(L->ext + (a ^ 1), qn, pid, r.cont || fresh, w.capacity, err);
   }
 }
 
@@ -545,7 +558,7 @@ cudaError_t launch_wave_chunk(const DevScene &s, const DevConfig &c, uint32_t pa
     if (sh_sorted) launch_sort(s, d - 1, w, kSortShadow, kShadowKeys, w.shadow_order, sort_grid, st);
     launch_trace(s, c, d, f, w, err, grid, block, st, trace_budget, ext_sorted, sh_sorted);
     if (sort_keys & 1) launch_sort(s, d, w, kSortShade, nmat, w.sorted, sort_grid, st);
-    k_shade<<<grid, block, 0, st>>>(s, c, pass, band, d, f, w, (sort_keys & 1) ? 1 : 0);
+    k_shade<<<grid, block, 0, st>>>(s, c, pass, band, d, f, w, (sort_keys & 1) ? 1 : 0, err);
   }
   // the last depth's shadow queries
   if (c.max_depth > 0) {
@@ -596,7 +609,7 @@ cudaError_t build_wave_loop(WaveLoopGraph &G, const DevScene &s, const DevConfig
       cudaSuccess)
     return e;
   launch_trace<true>(s, c, 0, f, w, err, grid, block, G.capture, budget, 0, 0, w.loop);
-  k_shade_loop<<<grid, block, 0, G.capture>>>(s, c, f, w, w.loop);
+  k_shade_loop<<<grid, block, 0, G.capture>>>(s, c, f, w, w.loop, err);
   k_loop_control<<<1, 32, 0, G.capture>>>(w.loop, h, 1, err);
   const cudaError_t le = cudaGetLastError();
   cudaGraph_t captured = nullptr;
@@ -610,7 +623,8 @@ cudaError_t build_wave_loop(WaveLoopGraph &G, const DevScene &s, const DevConfig
 
 cudaError_t launch_wave_loop(const DevScene &s, const DevConfig &c, uint32_t pass0, int band0, int npass, Film f,
                              const WaveBuffers &w, uint32_t *err, int grid, int block, cudaStream_t st,
-                             int trace_budget, int capacity, WaveLoopGraph **graph, bool host_driven) {
+                             int trace_budget, int capacity, WaveLoopGraph **graph, bool host_driven,
+                             int limit_override) {
   const int64_t npix = (int64_t)c.W * c.H;
   const int64_t total = npix * npass;
   if (c.max_depth > kMaxDepth || npass < 1 || npass > 32767 || capacity < 1 || capacity > w.capacity ||
@@ -621,7 +635,8 @@ cudaError_t launch_wave_loop(const DevScene &s, const DevConfig &c, uint32_t pas
   // every slot starts a new item at least once per max_depth iterations while
   // items are left, and a path lives at most max_depth iterations
   const int64_t bound = ((total + n0 - 1) / n0 + 2) * (int64_t)(c.max_depth + 1) + 4;
-  const int limit = (int)(bound < INT32_MAX ? bound : INT32_MAX);
+  int limit = (int)(bound < INT32_MAX ? bound : INT32_MAX);
+  if (limit_override > 0 && limit_override < limit) limit = limit_override;  // a caller's tighter bound
   const int shared = npass > 1 && s.num_eems > 0 ? 1 : 0;
   struct Key {
     DevScene s;
@@ -651,7 +666,7 @@ cudaError_t launch_wave_loop(const DevScene &s, const DevConfig &c, uint32_t pas
     k_loop_init<<<init_grid, 256, 0, st>>>(s, c, w, w.loop, pass0, band0, npass, n0, limit, shared);
     for (int it = 0; it < limit; ++it) {
       launch_trace<true>(s, c, 0, f, w, err, grid, block, st, trace_budget, 0, 0, w.loop);
-      k_shade_loop<<<grid, block, 0, st>>>(s, c, f, w, w.loop);
+      k_shade_loop<<<grid, block, 0, st>>>(s, c, f, w, w.loop, err);
       k_loop_control<<<1, 32, 0, st>>>(w.loop, 0, 0, err);
       int go = 0;
       cudaError_t e = cudaMemcpyAsync(&go, &w.loop->go, sizeof(int), cudaMemcpyDeviceToHost, st);
@@ -688,7 +703,11 @@ cudaError_t launch_wave_loop(const DevScene &s, const DevConfig &c, uint32_t pas
 // the work of one call: at most kNoAllocMaxPaths pixels (a tile of the frame).
 //
 // Every GPU that loads the library holds the array (about 8.4 MB) until the
-// process exits.  All calls share it: a call clears the counters it needs and
+// process exits.  The CUDA runtime loads the module that holds it lazily: the
+// array is reserved on a device by the first call of this entry point there
+// (or by an earlier launch of any wavefront kernel of this file), so a host
+// with a fixed memory budget makes that first call during start-up.  All calls
+// share it: a call clears the counters it needs and
 // overwrites the path state it uses, but two calls whose work overlaps on the
 // GPU (different streams, or different host threads on one device) race on
 // it and must be serialised by the caller.
@@ -723,9 +742,31 @@ __global__ void k_generate_tile(DevScene s, DevConfig c, uint32_t pass, int band
   if (blockIdx.x == 0 && threadIdx.x == 0) w.counts[kCntExt + 0] = n;
 }
 
-// device address of the scratch array, looked up once per device
+// Device address of the scratch array, looked up once per device and
+// context.  The address belongs to the context that loaded this module: after
+// a device reset (cudaDeviceReset, or a re-created primary context) the module
+// is loaded again elsewhere, so the cached address is keyed on the current
+// context and looked up again when it changes.
 std::mutex g_noalloc_mutex;
-void *g_noalloc_ptr[64] = {};
+struct NoallocSlot {
+  void *ctx = nullptr;  // CUcontext the address was looked up in
+  void *ptr = nullptr;
+};
+NoallocSlot g_noalloc[64];
+
+using CtxGetCurrentFn = int (*)(void **);  // cuCtxGetCurrent, reached through the runtime
+
+CtxGetCurrentFn ctx_get_current() {
+  static const CtxGetCurrentFn fn = [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &p, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return static_cast<CtxGetCurrentFn>(nullptr);
+    return reinterpret_cast<CtxGetCurrentFn>(p);
+  }();
+  return fn;
+}
 
 }  // namespace
 
@@ -735,15 +776,20 @@ size_t noalloc_scratch_bytes() { return kNoAllocScratchBytes; }
 cudaError_t noalloc_setup(int device, void **ptr) {
   if (device < 0 || device >= 64) return cudaErrorInvalidDevice;
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (!g_noalloc_ptr[device]) {
+  void *ctx = nullptr;
+  const CtxGetCurrentFn get = ctx_get_current();
+  const bool known = get && get(&ctx) == 0 && ctx;  // without a context id: look up on every call
+  NoallocSlot &slot = g_noalloc[device];
+  if (!known || !slot.ptr || slot.ctx != ctx) {
     // the host-side name of the array is only a stand-in; the kernels need
     // the address the device uses, looked up with the device current
     void *p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return e;
-    g_noalloc_ptr[device] = p;
+    slot.ptr = p;
+    slot.ctx = known ? ctx : nullptr;
   }
-  *ptr = g_noalloc_ptr[device];
+  *ptr = slot.ptr;
   return cudaSuccess;
 }
 
@@ -775,7 +821,7 @@ cudaError_t launch_wave_tile_noalloc(const DevScene &s, const DevConfig &c, uint
   k_generate_tile<<<(n + 255) / 256, 256, 0, st>>>(s, c, pass, band, w, x0, y0, tw, th);
   for (int d = 0; d < c.max_depth; ++d) {
     launch_trace(s, c, d, f, w, err, grid, block, st, trace_budget);
-    k_shade<<<grid, block, 0, st>>>(s, c, pass, band, d, f, w, 0);
+    k_shade<<<grid, block, 0, st>>>(s, c, pass, band, d, f, w, 0, err);
   }
   if (c.max_depth > 0) launch_trace(s, c, c.max_depth, f, w, err, grid, block, st, trace_budget);
   return cudaGetLastError();

@@ -265,6 +265,12 @@ class Renderer:
         self._check(self.lib.ts_wave_loop_iterations(self._ctx, _stream(), ctypes.byref(n)))
         return int(n.value)
 
+    def set_loop_iteration_limit(self, limit=0):
+        """Bound on the iterations of one regenerating-loop launch (0 = automatic);
+        a launch that reaches it stops on the device and check_device reports it."""
+        self.flush()
+        self._check(self.lib.ts_set_loop_iteration_limit(self._ctx, int(limit)))
+
     def cast_rays_counted(self, current_sample_in_block, pass_idx=None):
         """cast_rays through the counting megakernel; returns the work counts."""
         self.flush()

@@ -97,3 +97,37 @@ def test_renderer_refuses_to_run_without_gpu():
     s, c, ex = configs.box_scene(width=8, height=8)
     with pytest.raises(RuntimeError, match="no CPU fallback"):
         sb.Renderer(s, c, eems=ex["eems"], cmf=ex["cmf"])
+
+
+def integration_python_blocks():
+    """The ```python blocks of INTEGRATION.md."""
+    src = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    return re.findall(r"```python\n(.*?)```", src, flags=re.S)
+
+
+def test_integration_doc_structs_match_the_header():
+    """A host that copies INTEGRATION.md's ctypes binding gets structs of the
+    header's layout: every documented Structure class is executed and compared
+    field by field (name, size, offset) with include/spectral.h, and the
+    documented positional constructor fills every field."""
+    import ast
+    found = 0
+    for block in integration_python_blocks():
+        tree = ast.parse(block)
+        for node in tree.body:
+            if not (isinstance(node, ast.ClassDef) and node.name.startswith("ts_")):
+                continue
+            ns = {"ctypes": ctypes}
+            exec(compile(ast.Module(body=[node], type_ignores=[]), "INTEGRATION.md", "exec"), ns)
+            st = ns[node.name]
+            py = [(n, ctypes.sizeof(t)) for n, t in st._fields_]
+            assert py == header_struct(node.name), node.name
+            offs = [getattr(st, n).offset for n, _ in st._fields_]
+            assert offs == [sum(sz for _, sz in py[:i]) for i in range(len(py))], node.name
+            found += 1
+            # positional constructions in the same block give a value for every field
+            for call in ast.walk(tree):
+                if isinstance(call, ast.Call) and isinstance(call.func, ast.Name) and call.func.id == node.name \
+                        and call.args:
+                    assert len(call.args) == len(st._fields_), (node.name, len(call.args))
+    assert found >= 1

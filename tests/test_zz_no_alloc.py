@@ -60,6 +60,17 @@ def test_noalloc_rejects_oversized_and_out_of_frame_tiles():
         assert lib.ts_render_tile_noalloc(r._ctx, 0, 0, 0, 0, 300, 300, p, _stream()) == 4  # TS_ERR_CAPACITY
         assert b"65536" in lib.ts_last_error(r._ctx)
         assert lib.ts_render_tile_noalloc(r._ctx, 0, 0, 250, 0, 64, 64, p, _stream()) == 1  # outside the frame
-        assert lib.ts_render_tile_noalloc(r._ctx, 0, 0, 0, 0, 256, 256, p, _stream()) == 0  # exactly the limit
+        # exactly the limit: the whole scratch layout in use, against the regular pass on that region
+        assert lib.ts_render_tile_noalloc(r._ctx, 5, 11, 20, 30, 256, 256, p, _stream()) == 0
         torch.cuda.synchronize()
+        got = film.cpu().numpy()
+        r.clear_pixel_space()
+        r.cast_rays(11, pass_idx=5)
+        want = r.block_film.cpu().numpy()
+        tile = (slice(None), slice(30, 286), slice(20, 276))
+        assert np.count_nonzero(want[tile]) > 0
+        assert np.allclose(got[tile], want[tile], rtol=1e-12, atol=0.0)
+        outside = np.ones(got.shape, bool)
+        outside[tile] = False
+        assert not got[outside].any()  # nothing written outside the tile
         assert r.check_device() == 0
