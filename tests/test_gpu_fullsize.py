@@ -1,0 +1,153 @@
+"""Parity at the sizes the benchmark times.
+
+* Closest hits on the full large-mesh workload (the 2.59M-triangle terrain
+  of the bench, 1024x1024 camera) for every node width the autotuner may pick,
+  against the oracle's reference-order traversal (main.py:831-864): over a
+  million rays -- jittered camera rays of the whole frame, rays from above
+  the terrain in every direction (grazing ones included) and secondary rays
+  leaving the first hits -- the same triangle except counted near ties, hit
+  distances within 1e-5 relative; the exact-order kernel bit for bit.
+* The converged terrain image against the FP64 oracle image (64k spp on a
+  4096-pixel subset, independent random streams), rendered with the
+  benchmark's launch shape (regenerating wavefront loop, four-child nodes).
+* One scene of every generator kind of the batched workload (seeds 100..163),
+  rendered through both batch engines, against the oracle with the same
+  random streams.
+"""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from helpers import GOLDEN, camera_rays, orc, oracle_config, oracle_scene, sb
+from spectral_b200 import batch as sbatch
+from spectral_b200 import configs
+from test_gpu_trace import _near_tie_check, renderer_for
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def terrain():
+    s, c, ex = configs.terrain_scene()
+    comp = sb.compile_scene(s, c.bands, eems=ex["eems"], cmf=ex["cmf"])
+    bvh = sb._lib.build_bvh_host(comp.tris["v0"], comp.tris["v1"], comp.tris["v2"])
+    sc = oracle_scene(comp, bvh, s["camera"])
+    assert comp.num_tris > 2_500_000
+    rng = np.random.default_rng(11)
+    cam = camera_rays(s["camera"], c.width, c.height, fov_scale=c.fov_scale, jitter_seed=4)
+    n = 262144
+    o = np.stack([rng.uniform(-12, 12, n), rng.uniform(0.2, 6.0, n), rng.uniform(-12, 12, n)], 1)
+    d = rng.normal(size=(n, 3))
+    d[: n // 8, 1] *= 1e-3  # nearly horizontal: long grazing rays over the heightfield
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    above = np.concatenate([o, d], 1).astype(np.float32)
+    # secondary rays: from the oracle's first hits along the camera rays, random upper-hemisphere directions
+    sub = cam[rng.choice(cam.shape[0], n, replace=False)]
+    tri, t, _, _ = orc.trace(sc, oracle_config(sb.RenderConfig()), sub)
+    hit = tri >= 0
+    p = sub[hit, :3] + sub[hit, 3:] * (t[hit, None] * np.float32(0.9999))
+    d2 = rng.normal(size=p.shape)
+    d2[:, 1] = np.abs(d2[:, 1])
+    d2 /= np.linalg.norm(d2, axis=1, keepdims=True)
+    second = np.concatenate([p, d2], 1).astype(np.float32)
+    rays = np.concatenate([cam, above, second], 0)
+    tri_o, t_o, _, _ = orc.trace(sc, oracle_config(sb.RenderConfig()), rays)
+    perm = bvh["tri_perm"]
+    tri_o = np.where(tri_o >= 0, perm[np.maximum(tri_o, 0)], -1)
+    return dict(s=s, c=c, ex=ex, comp=comp, bvh=bvh, rays=rays, tri_o=tri_o, t_o=t_o)
+
+
+@pytest.mark.parametrize("node_width", [2, 4, 8])
+def test_full_size_terrain_closest_hits(terrain, node_width):
+    T = terrain
+    rays = T["rays"]
+    assert rays.shape[0] > 1_000_000
+    with renderer_for(T["comp"], T["bvh"], T["s"]["camera"], node_width=node_width) as r:
+        assert r.scene_info()["node_width"] == node_width
+        tri, t, _, _ = (x.cpu().numpy() for x in r.trace(torch.from_numpy(rays).cuda(), "fast"))
+        if node_width == 4:
+            k = 131072  # the exact reference-order kernel on a share of the rays
+            tri_e, t_e, _, _ = (x.cpu().numpy() for x in r.trace(torch.from_numpy(rays[:k]).cuda(),
+                                                                  "reference_order"))
+            assert np.array_equal(tri_e, T["tri_o"][:k]) and np.array_equal(t_e, T["t_o"][:k])
+        assert r.check_device() == 0
+    ties = _near_tie_check(tri, t, T["tri_o"], T["t_o"])
+    assert ties <= 0.002 * len(rays), ties
+    assert 0.3 < (T["tri_o"] >= 0).mean() < 0.95
+
+
+def test_terrain_converged_within_3_sigma():
+    """The bench workload's image after 400 blocks (10,000 spp) against the FP64
+    oracle image: the per-cell 3-sigma band holds on >= 95 % of the subset's
+    cells (heavy-tailed firefly paths of the small lights on glossy conductors
+    make the per-cell estimate of the standard error itself noisy) and the
+    image total within 4 combined standard errors."""
+    d = dict(np.load(os.path.join(GOLDEN, "oracle_terrain.npz")))
+    s, c, ex = configs.terrain_scene()
+    B = c.bands
+    c.kernel = "wavefront"
+    c.queue_capacity = B * c.width * c.height
+    c.trace_budget = 16
+    blocks = 400
+    with sb.Renderer(s, c, eems=ex["eems"], cmf=ex["cmf"], bvh_params={"width": 4}) as r:
+        for b in range(blocks):
+            r.cast_rays_bundle(0, B, pass_idx=b * B)
+            r.average_and_reset_block(b + 1)
+        pix = torch.as_tensor(d["pixels"].astype(np.int64), device="cuda")
+        mean = r.mean_film.reshape(B, -1)[:, pix].T.cpu().numpy()
+        m2 = r.m2_film.reshape(B, -1)[:, pix].T.cpu().numpy()
+        assert r.check_device() == 0
+    n = blocks
+    sem = np.sqrt(np.maximum(m2 / n - mean * mean, 0) / (n - 1))
+    diff = mean - d["mean"].astype(np.float64)
+    tot = np.sqrt(sem ** 2 + d["sem"].astype(np.float64) ** 2)
+    ok = np.abs(diff) <= 3 * tot + 1e-12
+    assert ok.mean() >= 0.95, ok.mean()
+    assert abs(diff.sum()) <= 4 * np.sqrt((tot ** 2).sum()), (diff.sum(), np.sqrt((tot ** 2).sum()))
+
+
+def _first_of_each_kind():
+    seen = {}
+    for seed in range(100, 164):
+        out = configs.batch_scene(seed)
+        kind = out[2]["kind"]
+        if kind not in seen:
+            seen[kind] = out
+        if len(seen) == 3:
+            break
+    return [seen[k] for k in ("box", "terrain", "volume")]
+
+
+@pytest.mark.parametrize("engine", ["kernel", "streams"])
+def test_batched_scenes_of_every_kind_match_oracle(engine):
+    scenes = _first_of_each_kind()
+    rs, oracles = [], []
+    for i, (s, c, ex) in enumerate(scenes):
+        c.kernel = "mega"
+        c.scene_id = 7 + i  # distinct random streams per scene, as a batch keys them
+        comp = sb.compile_scene(s, c.bands, eems=ex["eems"], cmf=ex["cmf"])
+        bvh = sb._lib.build_bvh_host(comp.tris["v0"], comp.tris["v1"], comp.tris["v2"])
+        rs.append(sb.Renderer(s, c, eems=ex["eems"], cmf=ex["cmf"], bvh=bvh))
+        oracles.append((oracle_scene(comp, bvh, s["camera"]), oracle_config(c, scene_id=c.scene_id)))
+    try:
+        B = rs[0].config.bands
+        first = 300
+        with (sbatch.Batch(rs, use_graph=True) if engine == "kernel" else sbatch.StreamBatch(rs, streams=4)) as b:
+            b.reset(first_pass=first)
+            b.step()  # one block of every scene, then its block average (n = 1)
+            assert b.check() == 0
+            for r, (osc, ocf) in zip(rs, oracles):
+                npix = r.config.width * r.config.height
+                pix = np.sort(np.random.default_rng(5).choice(npix, min(2048, npix), replace=False)).astype(np.int32)
+                ref = np.zeros((len(pix), B))
+                for k in range(B):
+                    orc.render_pass(osc, ocf, first + k, k, pix, out=ref)
+                got = r.mean_film.reshape(B, -1)[:, torch.as_tensor(pix.astype(np.int64), device="cuda")].T
+                got = got.cpu().numpy()
+                assert np.isclose(got, ref, rtol=1e-3, atol=1e-7).mean() > 0.995, r.config.width
+                assert abs(got.sum() - ref.sum()) <= 2e-3 * abs(ref.sum()) + 1e-9
+    finally:
+        for r in rs:
+            r.close()
