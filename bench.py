@@ -336,13 +336,26 @@ def adjoint_leg():
     n = 2 * B
     f1 = timed(lambda: [r.cast_rays(p % B, pass_idx=1000 + p) for p in range(n)], n)
     fb = timed(lambda: [r.cast_rays_bundle(0, B, pass_idx=1000 + i * B) for i in range(2)], n)
-    ab = timed(lambda: r.adjoint_passes(0, n, 1000, adj, g), n)
+    ab = timed(lambda: r.adjoint_passes(0, n, 1000, adj, g), n)  # both replays
+    # the inverse workflow: the forward bundles record each path's total deposit,
+    # the adjoint of the same passes then needs one replay per path
+    r.record_paths(2000, n)
+    fr = timed(lambda: [r.cast_rays_bundle(0, B, pass_idx=2000 + i * B) for i in range(2)], n)
+    ar = timed(lambda: r.adjoint_passes(0, n, 2000, adj, g), n)
+    r.record_paths(0, 0)
     bits = r.check_device()
     r.close()
     return {"workload": "inverse-rendering scene: box + 20k-tri HG medium (g 0.7) + fluorescent wall, 256x256, "
                         "depth 32, 25 bands; parameters " + str(pm + pe),
-            "forward_ms_per_pass": f1, "forward_bundle_ms_per_pass": fb, "adjoint_ms_per_pass": ab,
-            "adjoint_over_forward": ab / f1, "adjoint_over_forward_bundle": ab / fb, "device_error_bits": bits}
+            "forward_ms_per_pass": f1, "forward_bundle_ms_per_pass": fb,
+            "forward_bundle_recorded_ms_per_pass": fr, "adjoint_ms_per_pass": ar,
+            "adjoint_two_replays_ms_per_pass": ab,
+            "adjoint_over_forward": ar / f1, "adjoint_over_forward_bundle": ar / fb,
+            "adjoint_over_recorded_forward_bundle": ar / fr,
+            "what": "adjoint of passes whose forward bundles recorded each path's total deposit (ts_record_paths: "
+                    "one gradient replay per path); adjoint_two_replays_ms_per_pass is the same adjoint without "
+                    "records (weight replay + gradient replay)",
+            "device_error_bits": bits}
 
 
 def bench_adjoint(args):

@@ -235,6 +235,17 @@ ts_status ts_param_count(const ts_ctx *ctx, int64_t *num_material_params, int64_
  * surface_emission) and EEM ids stay as uploaded.  Stream-ordered. */
 ts_status ts_update_materials(ts_ctx *ctx, const float *mat_f32_dev, const float *eem_dev, void *stream);
 
+/* Path records (new): arm recording for passes first_pass .. first_pass +
+ * num_passes - 1 (num_passes = 0 disarms; allocates num_passes * W * H floats
+ * here, not while rendering).  Renders of armed passes (ts_render_pass, and
+ * ts_render_passes whose passes all fall in the range) run the megakernel and
+ * write each path's total deposit.  A later ts_adjoint_passes over recorded
+ * passes at the same bands then skips its weight replay for every path that
+ * stayed in its band (the weight is the adjoint film at the path's cell times
+ * the recorded total); the gradients are the same.  Uploading a scene, moving
+ * the camera or updating the materials marks the records stale. */
+ts_status ts_record_paths(ts_ctx *ctx, uint32_t first_pass, int32_t num_passes);
+
 /* Path-replay adjoint of ts_render_pass(pass_idx, band): re-runs each path of
  * that pass from its random stream and ADDS into grad_dev ([M*6*B + E*B*B]
  * float64, device) the derivative of sum over the pass's film deposits of

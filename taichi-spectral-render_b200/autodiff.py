@@ -11,9 +11,11 @@ path-replay adjoint kernel of libspectral.so (ts_adjoint_pass):
 
 Forward renders ``num_blocks`` whole spectral blocks (pass i renders band
 i mod B with random stream first_pass + i) and returns the running mean over
-blocks, as average_and_reset_block leaves it (main.py:1592-1607).  Backward
-re-runs exactly those paths from their random streams and accumulates the
-gradient in FP64.  Gradients exist for every table entry except the
+blocks, as average_and_reset_block leaves it (main.py:1592-1607); it records
+each path's total deposit (ts_record_paths).  Backward re-runs exactly those
+paths from their random streams and accumulates the gradient in FP64; with the
+forward's records it needs one replay per path, not two (a path that volume
+fluorescence moved to another band is replayed twice).  Gradients exist for every table entry except the
 refractive index (property 0), which is returned as zero.
 """
 import torch
@@ -28,6 +30,7 @@ class _RenderFilm(torch.autograd.Function):
         r.update_materials(mat, em)
         r.clear_pixel_space()
         B = r.config.bands
+        r.record_paths(first_pass, num_blocks * B)  # the adjoint then skips its weight replay
         for blk in range(num_blocks):
             r.cast_rays_bundle(0, B, pass_idx=first_pass + blk * B)  # one launch per block
             r.average_and_reset_block(blk + 1)
@@ -38,6 +41,7 @@ class _RenderFilm(torch.autograd.Function):
         ctx.has_eem = eem is not None
         ctx.mat_dtype = mat_f32.dtype
         ctx.eem_dtype = None if eem is None else eem.dtype
+        ctx.materials_version = r.materials_version
         ctx.save_for_backward(mat, em if em is not None else mat.new_empty(0))
         return film
 
@@ -46,7 +50,9 @@ class _RenderFilm(torch.autograd.Function):
         r = ctx.renderer
         mat, em = ctx.saved_tensors
         # the adjoint replays the forward pass's paths: same tables, same streams
-        r.update_materials(mat, em if ctx.has_eem else None)
+        # (re-uploaded only if they changed since, which also retires the records)
+        if r.materials_version != ctx.materials_version:
+            r.update_materials(mat, em if ctx.has_eem else None)
         adj = (grad_film.to(r.device, torch.float64) / ctx.num_blocks).contiguous()
         pm, pe = r.param_count()
         grad = torch.zeros(pm + pe, dtype=torch.float64, device=r.device)

@@ -209,7 +209,8 @@ template <int W, int kPhase>
 __global__ void __launch_bounds__(128, kPhase ? 4 : 5) k_adjoint(DevScene s, DevConfig c, uint32_t pass0, int npass, int band0,
                                                  const double *__restrict__ adj, double *__restrict__ grad,
                                                  float *__restrict__ weight, int pm_shared, int pmat,
-                                                 int *__restrict__ counter, uint32_t *__restrict__ err) {
+                                                 int *__restrict__ counter, uint32_t *__restrict__ err,
+                                                 const float *__restrict__ rec) {
   extern __shared__ double sh_grad[];
   for (int i = threadIdx.x; i < pm_shared; i += blockDim.x) sh_grad[i] = 0.0;
   __syncthreads();
@@ -249,17 +250,26 @@ __global__ void __launch_bounds__(128, kPhase ? 4 : 5) k_adjoint(DevScene s, Dev
           band = (band0 + po) % B;
           item = idx;
           atot = 0.f;
-          if (phase) arem = weight[idx];
-          rng.init(c.seed, pass, (uint32_t)pix, c.scene_id);
-          camera_ray(s, c, pix % c.W, pix / c.W, rng, p, band);
-          sp.reset();
-          k = 0;
+          const float r = !phase && rec ? rec[idx] : -1.f;
+          if (r >= 0.f) {
+            // the forward pass recorded this path's total deposit, all of it in
+            // its own band: A = w(pixel, band) * total, no replay needed
+            weight[idx] = (float)__ldg(adj + (size_t)band * npix + pix) * r;
+            pix = -1;
+          } else {
+            if (phase) arem = weight[idx];
+            rng.init(c.seed, pass, (uint32_t)pix, c.scene_id);
+            camera_ray(s, c, pix % c.W, pix / c.W, rng, p, band);
+            sp.reset();
+            k = 0;
+          }
         } else {
           exhausted = true;
         }
       }
     }
-    if (__ballot_sync(0xffffffffu, pix >= 0) == 0) break;
+    // lanes that took a recorded item fetch again; stop when every lane is idle and out of items
+    if (__ballot_sync(0xffffffffu, pix >= 0 || !exhausted) == 0) break;
     if (pix < 0) continue;
 
     // ---- one path vertex, exactly as the forward megakernel takes it
@@ -398,27 +408,27 @@ namespace {
 template <int W>
 void launch_pair(const DevScene &s, const DevConfig &c, uint32_t pass, int npass, int band, const double *adj,
                  double *grad, float *weight, int psh, int pmat, int *counter, uint32_t *err, int grid,
-                 cudaStream_t st) {
+                 cudaStream_t st, const float *rec) {
   const int block = 128;
-  k_adjoint<W, 0><<<grid, block, 0, st>>>(s, c, pass, npass, band, adj, grad, weight, 0, pmat, counter, err);
+  k_adjoint<W, 0><<<grid, block, 0, st>>>(s, c, pass, npass, band, adj, grad, weight, 0, pmat, counter, err, rec);
   k_adjoint<W, 1><<<grid, block, (size_t)psh * sizeof(double), st>>>(s, c, pass, npass, band, adj, grad, weight, psh,
-                                                                     pmat, counter + 1, err);
+                                                                     pmat, counter + 1, err, nullptr);
 }
 }  // namespace
 
 cudaError_t launch_adjoint(const DevScene &s, const DevConfig &c, uint32_t pass, int band, const double *adj,
                            double *grad, float *weight, int *counter, uint32_t *err, int grid, cudaStream_t st,
-                           int npass) {
+                           int npass, const float *rec) {
   cudaError_t e = cudaMemsetAsync(counter, 0, 2 * sizeof(int), st);
   if (e != cudaSuccess) return e;
   const int pmat = s.num_materials * 6 * c.B;
   const int psh = adjoint_shared_params(pmat);
-  if (s.node_width == 8) launch_pair<8>(s, c, pass, npass, band, adj, grad, weight, psh, pmat, counter, err, grid, st);
+  if (s.node_width == 8) launch_pair<8>(s, c, pass, npass, band, adj, grad, weight, psh, pmat, counter, err, grid, st, rec);
   else if (s.node_width == 4)
-    launch_pair<4>(s, c, pass, npass, band, adj, grad, weight, psh, pmat, counter, err, grid, st);
+    launch_pair<4>(s, c, pass, npass, band, adj, grad, weight, psh, pmat, counter, err, grid, st, rec);
   else if (c.speculative)
-    launch_pair<3>(s, c, pass, npass, band, adj, grad, weight, psh, pmat, counter, err, grid, st);
-  else launch_pair<2>(s, c, pass, npass, band, adj, grad, weight, psh, pmat, counter, err, grid, st);
+    launch_pair<3>(s, c, pass, npass, band, adj, grad, weight, psh, pmat, counter, err, grid, st, rec);
+  else launch_pair<2>(s, c, pass, npass, band, adj, grad, weight, psh, pmat, counter, err, grid, st, rec);
   return cudaGetLastError();
 }
 

@@ -48,6 +48,13 @@ struct ts_ctx {
   std::vector<void *> wave_allocs;
   ts::WaveLoopGraph *wave_loop = nullptr;  // captured regenerating wavefront loop
   int loop_limit = 0;                      // caller's bound on loop iterations per launch (0 = automatic)
+  // path records for the adjoint (ts_record_paths): per path of the armed
+  // passes its total deposit, written by megakernel renders of those passes
+  float *d_rec = nullptr;
+  size_t rec_cap = 0;              // entries allocated
+  uint32_t rec_first = 0;          // first pass of the armed range
+  int rec_num = 0;                 // passes in the armed range (0 = not armed)
+  std::vector<int> rec_band;       // per pass of the range: band it was recorded at (-1 = not recorded)
   size_t film_bytes = 0, scene_bytes = 0, wave_bytes = 0;
   float cam[9] = {0, 0, 3.5f, 0, 0, -1, 0, 1, 0};
   std::string err;
@@ -221,6 +228,8 @@ ts_status ts_set_launch_config(ts_ctx *c, const ts_config *k) {
   return TS_OK;
 }
 
+static void rec_invalidate(ts_ctx *c);
+
 ts_status ts_destroy(ts_ctx *c) {
   if (!c) return TS_OK;
   cudaSetDevice(c->cfg.device);
@@ -233,12 +242,14 @@ ts_status ts_destroy(ts_ctx *c) {
   cudaFree(c->d_xyz);
   cudaFree(c->d_m9);
   cudaFree(c->d_adj_weight);
+  cudaFree(c->d_rec);
   delete c;
   return TS_OK;
 }
 
 ts_status ts_upload_scene(ts_ctx *c, const ts_scene_desc *sd) {
   if (!c || !sd) return fail(c, TS_ERR_INVALID_ARG, "ts_upload_scene: null argument");
+  rec_invalidate(c);
   cudaSetDevice(c->cfg.device);
   const int T = sd->num_tris, M = sd->num_materials, B = c->cfg.bands, E = sd->num_eems;
   if (T < 0 || (T > 0 && (!sd->v0 || !sd->v1 || !sd->v2 || !sd->n0 || !sd->n1 || !sd->n2 || !sd->normal ||
@@ -478,6 +489,7 @@ ts_status ts_build_bvh_host(int32_t T, const float *v0, const float *v1, const f
 ts_status ts_set_camera(ts_ctx *c, const float o[3], const float l[3], const float up[3]) {
   if (!c || !o || !l || !up) return fail(c, TS_ERR_INVALID_ARG, "ts_set_camera: null argument");
   float tmp[9] = {o[0], o[1], o[2], l[0], l[1], l[2], up[0], up[1], up[2]};
+  if (std::memcmp(tmp, c->cam, sizeof(tmp)) != 0) rec_invalidate(c);
   std::memcpy(c->cam, tmp, sizeof(tmp));
   float3 w, u, v;
   camera_basis(o, l, up, w, u, v);
@@ -507,6 +519,66 @@ static ts_status render_wave_loop(ts_ctx *c, uint32_t pass0, int npass, int band
   return TS_OK;
 }
 
+// ---- path records (ts_record_paths)
+// records of passes [p0, p0 + n) when all of them fall inside the armed range
+static float *rec_slot(ts_ctx *c, uint32_t p0, int n) {
+  if (c->rec_num <= 0) return nullptr;
+  const uint32_t off = p0 - c->rec_first;  // unsigned: passes before the range wrap to large offsets
+  if (off >= (uint32_t)c->rec_num || (int64_t)off + n > c->rec_num) return nullptr;
+  return c->d_rec + (size_t)off * c->cfg.width * c->cfg.height;
+}
+
+// every pass of [p0, p0 + n) recorded at the bands an adjoint starting at band0 replays
+static bool rec_current(ts_ctx *c, uint32_t p0, int n, int band0) {
+  if (!rec_slot(c, p0, n)) return false;
+  const uint32_t off = p0 - c->rec_first;
+  for (int i = 0; i < n; ++i)
+    if (c->rec_band[off + i] != (band0 + i) % c->cfg.bands) return false;
+  return true;
+}
+
+// anything that changes a pass's paths makes the records stale
+static void rec_invalidate(ts_ctx *c) { std::fill(c->rec_band.begin(), c->rec_band.end(), -1); }
+
+// a megakernel launch of npass passes that also writes their path records
+static ts_status render_recorded(ts_ctx *c, uint32_t pass0, int npass, int band0, float *rec, cudaStream_t st,
+                                 const char *what) {
+  const int bs = c->cfg.block_size;
+  int per_sm = c->cfg.blocks_per_sm;
+  if (per_sm <= 0) per_sm = std::max(1, 2048 / bs);
+  ts::Film f = film_of(c);
+  f.rec = rec;
+  TS_CUDA(c, ts::launch_render_mega(c->ds, c->dc, pass0, band0, f, c->d_counter, c->d_err, c->num_sms * per_sm, bs, st,
+                                    nullptr, npass, c->cfg.occupancy),
+          what);
+  const uint32_t off = pass0 - c->rec_first;
+  for (int i = 0; i < npass; ++i) c->rec_band[off + i] = (band0 + i) % c->cfg.bands;
+  return TS_OK;
+}
+
+ts_status ts_record_paths(ts_ctx *c, uint32_t first_pass, int32_t num_passes) {
+  if (!c) return fail(nullptr, TS_ERR_INVALID_ARG, "ts_record_paths: null context");
+  if (num_passes < 0) return fail(c, TS_ERR_INVALID_ARG, "ts_record_paths: num_passes must be >= 0");
+  c->rec_num = 0;
+  c->rec_band.clear();
+  if (num_passes == 0) return TS_OK;
+  const int64_t need = (int64_t)num_passes * c->cfg.width * c->cfg.height;
+  if (need > ((int64_t)1 << 30))
+    return fail(c, TS_ERR_CAPACITY, "ts_record_paths: more than 2^30 paths (4 GB of records)");
+  cudaSetDevice(c->cfg.device);
+  if ((size_t)need > c->rec_cap) {
+    cudaFree(c->d_rec);
+    c->d_rec = nullptr;
+    c->rec_cap = 0;
+    TS_CUDA(c, cudaMalloc((void **)&c->d_rec, (size_t)need * sizeof(float)), "ts_record_paths");
+    c->rec_cap = (size_t)need;
+  }
+  c->rec_first = first_pass;
+  c->rec_num = num_passes;
+  c->rec_band.assign(num_passes, -1);
+  return TS_OK;
+}
+
 ts_status ts_render_pass(ts_ctx *c, uint32_t pass_idx, int32_t band, void *stream) {
   if (!c) return fail(nullptr, TS_ERR_INVALID_ARG, "ts_render_pass: null context");
   if (!c->has_scene) return fail(c, TS_ERR_NO_SCENE, "ts_render_pass: no scene uploaded");
@@ -514,6 +586,7 @@ ts_status ts_render_pass(ts_ctx *c, uint32_t pass_idx, int32_t band, void *strea
   cudaSetDevice(c->cfg.device);
   const cudaStream_t st = as_stream(stream);
   const int bs = c->cfg.block_size;
+  if (float *rec = rec_slot(c, pass_idx, 1)) return render_recorded(c, pass_idx, 1, band, rec, st, "render pass");
   if (c->cfg.kernel == TS_KERNEL_MEGA) {
     int per_sm = c->cfg.blocks_per_sm;
     if (per_sm <= 0) per_sm = std::max(1, 2048 / bs);
@@ -545,6 +618,10 @@ ts_status ts_render_passes(ts_ctx *c, uint32_t first_pass, int32_t num_passes, i
     return fail(c, TS_ERR_INVALID_ARG, "ts_render_passes: num_passes must be 1..bands (one film plane per pass)");
   if ((int64_t)num_passes * c->cfg.width * c->cfg.height > INT32_MAX)
     return fail(c, TS_ERR_CAPACITY, "ts_render_passes: more than 2^31 paths in one launch");
+  if (float *rec = rec_slot(c, first_pass, num_passes)) {
+    cudaSetDevice(c->cfg.device);
+    return render_recorded(c, first_pass, num_passes, first_band, rec, as_stream(stream), "ts_render_passes");
+  }
   if (c->cfg.kernel != TS_KERNEL_MEGA && c->cfg.sort_keys == 0) {
     cudaSetDevice(c->cfg.device);
     const ts_status s = ensure_wave(c);
@@ -738,6 +815,7 @@ ts_status ts_update_materials(ts_ctx *c, const float *mat_f32_dev, const float *
   if (eem_dev && c->ds.num_eems <= 0)
     return fail(c, TS_ERR_INVALID_ARG, "ts_update_materials: the scene has no EEM table");
   cudaSetDevice(c->cfg.device);
+  rec_invalidate(c);
   TS_CUDA(c, ts::launch_update_materials(c->d_mat, mat_f32_dev, c->ds.num_materials, c->cfg.bands, c->d_eem, c->d_qy,
                                          c->d_cdf, eem_dev, c->ds.num_eems, as_stream(stream)),
           "ts_update_materials");
@@ -776,8 +854,12 @@ ts_status ts_adjoint_passes(ts_ctx *c, uint32_t first_pass, int32_t num_passes, 
   }
   for (int64_t p0 = 0; p0 < num_passes; p0 += chunk) {
     const int n = (int)std::min<int64_t>(chunk, num_passes - p0);
-    TS_CUDA(c, ts::launch_adjoint(c->ds, c->dc, first_pass + (uint32_t)p0, (int)((band + p0) % c->cfg.bands), adj_dev,
-                                  grad_dev, c->d_adj_weight, c->d_counter, c->d_err, grid, as_stream(stream), n),
+    const uint32_t cp = first_pass + (uint32_t)p0;
+    const int cb = (int)((band + p0) % c->cfg.bands);
+    // paths the forward pass recorded skip the weight replay
+    const float *rec = rec_current(c, cp, n, cb) ? rec_slot(c, cp, n) : nullptr;
+    TS_CUDA(c, ts::launch_adjoint(c->ds, c->dc, cp, cb, adj_dev, grad_dev, c->d_adj_weight, c->d_counter, c->d_err,
+                                  grid, as_stream(stream), n, rec),
             "ts_adjoint_pass");
   }
   return TS_OK;

@@ -14,6 +14,10 @@ struct Film {
   double *mean;   // running mean over completed blocks (spectral_accumulator)
   double *m2;     // sum over blocks of block^2 (for the per-pixel standard error)
   int W, H, B;
+  // path records for the adjoint (megakernel only; nullptr = none): per work
+  // item of the launch the path's total deposit, or -1 where volume
+  // fluorescence moved the path to another band
+  float *rec = nullptr;
 };
 
 // npass consecutive sample passes (cast_rays) from pass / band, band wrapping
@@ -97,7 +101,7 @@ int adjoint_shared_params(int pmat);
 constexpr int kAdjMaxPathsPerLaunch = 1 << 24;  // bounds the weight scratch at 64 MB
 cudaError_t launch_adjoint(const DevScene &s, const DevConfig &c, uint32_t pass, int band, const double *adj,
                            double *grad, float *weight, int *counter, uint32_t *err, int grid, cudaStream_t st,
-                           int npass = 1);
+                           int npass = 1, const float *rec = nullptr);
 // repack material [M][6][B] and/or EEM [E][B][B] tables given as device arrays
 cudaError_t launch_update_materials(float4 *mat, const float *mat_f32, int M, int B, float *eem, float *qy,
                                     float *cdf, const float *eem_src, int E, cudaStream_t st);

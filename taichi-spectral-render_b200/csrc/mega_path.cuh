@@ -24,6 +24,8 @@ struct MegaLane {
   int band;    // the pass's band (transport band)
   int k;       // loop iteration
   double dep;  // pending deposit into p.active_px
+  int item;    // work item of the launch (index of its path record)
+  bool moved;  // volume fluorescence moved the path to another band
 };
 
 // work counters of the counting variant (algorithmic bytes of the roofline)
@@ -41,8 +43,10 @@ __device__ __forceinline__ void mega_flush(const Film &f, int pixel, int band, d
 }
 
 __device__ __forceinline__ void mega_start(const DevScene &s, const DevConfig &c, MegaLane &L, uint32_t pass,
-                                           int band, int pixel) {
+                                           int band, int pixel, int item = 0) {
   L.pix = pixel;
+  L.item = item;
+  L.moved = false;
   L.band = band;
   L.rng.init(c.seed, pass, (uint32_t)pixel, c.scene_id);
   camera_ray(s, c, pixel % c.W, pixel / c.W, L.rng, L.p, band);
@@ -114,6 +118,7 @@ __device__ __forceinline__ bool mega_vertex(const DevScene &s, const DevConfig &
       if (kCount) cnt.dep += L.dep != 0.0;
       mega_flush(f, L.pix, p.active_px, L.dep, shared);
       L.dep = 0.0;
+      L.moved = true;
       p.active = ev.new_wl;
       p.active_px = ev.new_wl;
       p.plen++;
@@ -127,6 +132,8 @@ __device__ __forceinline__ bool mega_vertex(const DevScene &s, const DevConfig &
   if (done) {
     if (kCount) cnt.dep += L.dep != 0.0;
     mega_flush(f, L.pix, p.active_px, L.dep, shared);
+    // the adjoint's replay 0 reads a recorded total instead of re-tracing the path
+    if (f.rec) f.rec[L.item] = L.moved ? -1.0f : (float)L.dep;
     L.pix = -1;
   }
   return done;

@@ -48,7 +48,7 @@ __global__ void __launch_bounds__(128, kMinBlocks) k_render_mega(DevScene s, Dev
           int band = band0 + po;
           if (band >= c.B) band -= c.B;
           if (kCount) cnt.paths++;
-          mega_start(s, c, L, pass0 + (uint32_t)po, band, idx - po * npix);
+          mega_start(s, c, L, pass0 + (uint32_t)po, band, idx - po * npix, idx);
         } else {
           exhausted = true;
         }

@@ -265,6 +265,14 @@ class Renderer:
         self._check(self.lib.ts_wave_loop_iterations(self._ctx, _stream(), ctypes.byref(n)))
         return int(n.value)
 
+    def record_paths(self, first_pass=0, num_passes=0):
+        """Arm path records for passes first_pass .. first_pass + num_passes - 1
+        (0 disarms): renders of those passes run the megakernel and record each
+        path's total deposit, which a later adjoint of the same passes uses in
+        place of its weight replay."""
+        self.flush()
+        self._check(self.lib.ts_record_paths(self._ctx, int(first_pass) & 0xFFFFFFFF, int(num_passes)))
+
     def set_loop_iteration_limit(self, limit=0):
         """Bound on the iterations of one regenerating-loop launch (0 = automatic);
         a launch that reaches it stops on the device and check_device reports it."""
@@ -452,6 +460,7 @@ class Renderer:
         if eem is not None and tuple(eem.shape) != (E, B, B):
             raise ValueError(f"eem must be [{E}, {B}, {B}]")
         self._check(self.lib.ts_update_materials(self._ctx, p(mat_f32), p(eem), _stream()))
+        self.materials_version = getattr(self, "materials_version", 0) + 1
 
     def adjoint_pass(self, current_sample_in_block, pass_idx, adj, grad):
         """Path-replay adjoint of cast_rays(current_sample_in_block, pass_idx=pass_idx).

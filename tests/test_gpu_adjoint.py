@@ -173,3 +173,48 @@ def test_update_materials_replaces_tables():
         assert torch.allclose(render(), 2.0 * a, rtol=1e-6, atol=0)
         with pytest.raises(ValueError):
             r.update_materials(mat[:, :5].contiguous(), None)
+
+
+@pytest.mark.parametrize("fluorescent", [False, True])
+def test_recorded_forward_gives_the_same_gradient(fluorescent):
+    """ts_record_paths: the adjoint of passes whose forward render recorded each
+    path's total skips the weight replay for paths that stayed in their band
+    (all of them without a fluorescent medium; the moved ones are replayed) --
+    the same gradient as the two-replay adjoint, also after the records went
+    stale (camera moved and back)."""
+    from spectral_b200 import configs
+    s, c, ex = configs.volume_scene(width=24, height=24, medium_slices=12, medium_stacks=13, depth=9,
+                                    fluorescent_medium=fluorescent)
+    c.kernel = "wavefront"  # recorded renders take the megakernel whatever the launch settings
+    with sb.Renderer(s, c, eems=ex["eems"], cmf=ex["cmf"]) as r:
+        B = c.bands
+        pm, pe = r.param_count()
+        adj = torch.rand((B, c.height, c.width), dtype=torch.float64, device="cuda")
+        g0 = torch.zeros(pm + pe, dtype=torch.float64, device="cuda")
+        r.adjoint_passes(0, 2 * B, 100, adj, g0)
+        r.record_paths(100, 2 * B)
+        for blk in range(2):
+            r.cast_rays_bundle(0, B, pass_idx=100 + blk * B)
+        film_rec = r.block_film.clone()
+        g1 = torch.zeros_like(g0)
+        r.adjoint_passes(0, 2 * B, 100, adj, g1)
+        assert r.check_device() == 0
+        scale = g0.abs().max()
+        assert scale > 0
+        assert torch.allclose(g1, g0, rtol=1e-4, atol=1e-7 * float(scale))
+        # recording changed no image: the same passes without records
+        r.record_paths(0, 0)
+        r.clear_pixel_space()
+        for blk in range(2):
+            r.cast_rays_bundle(0, B, pass_idx=100 + blk * B)
+        assert torch.allclose(r.block_film, film_rec, rtol=1e-12, atol=0)
+        # stale records are not used
+        r.record_paths(100, 2 * B)
+        for blk in range(2):
+            r.cast_rays_bundle(0, B, pass_idx=100 + blk * B)
+        cam = s["camera"]
+        r.update_camera([0.0, 0.1, 0.45], cam["lookat"], cam["up"])
+        r.update_camera(cam["origin"], cam["lookat"], cam["up"])
+        g2 = torch.zeros_like(g0)
+        r.adjoint_passes(0, 2 * B, 100, adj, g2)
+        assert torch.allclose(g2, g0, rtol=1e-9, atol=1e-12 * float(scale))  # FP64 atomics in another order
