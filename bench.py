@@ -44,7 +44,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--kernel", default="mega", choices=["mega", "wavefront"])
-    p.add_argument("--workload", default="terrain", choices=["terrain", "box", "volume", "batch", "adjoint"])
+    p.add_argument("--workload", default="terrain", choices=["terrain", "box", "volume", "batch", "adjoint", "rmse"])
     p.add_argument("--width", type=int, default=2, choices=[2, 4, 8], help="BVH node width")
     p.add_argument("--traversal", default="default", choices=["default", "speculative"])
     p.add_argument("--occupancy", type=int, default=0, choices=[0, 8], help="megakernel register budget (--no-tune)")
@@ -60,6 +60,8 @@ def parse():
     p.add_argument("--no-tune", action="store_true", help="use --kernel/--width/--traversal as given instead of "
                                                           "the autotuner's choice")
     p.add_argument("--rmse-seconds", type=float, default=60.0, help="time limit of each time-to-RMSE leg")
+    p.add_argument("--rmse-target", type=float, default=0.01, help="relative XYZ RMSE target (--workload rmse)")
+    p.add_argument("--rmse-workloads", default="box,terrain,volume", help="workloads of --workload rmse")
     p.add_argument("--batch-scenes", type=int, default=64, help="scenes of the batched workload (--workload batch)")
     p.add_argument("--batch-target", type=float, default=0.05, help="RMSE target of the batched workload")
     p.add_argument("--passes", type=int, default=25, help="passes per adjoint launch (--workload adjoint)")
@@ -305,6 +307,62 @@ def rmse_leg(name, target, seconds, bundles=True):
     r.close()
     out["device_error_bits"] = bits
     return out
+
+
+def plain_seconds(name, blocks, timed_blocks=6):
+    """The plain single-scene kernel -- the depth-synchronous wavefront pass,
+    one launch per pass, no bundles -- on the first blocks of a time-to-RMSE
+    leg (the same passes, so the same paths and the same image): seconds per
+    block from CUDA events over ``timed_blocks`` blocks, and the seconds the
+    leg's ``blocks`` take at that rate."""
+    import torch
+    import spectral_b200 as sb
+    scene, cfg, ex, desc = workload(name)
+    cfg.kernel = "wavefront"
+    cfg.queue_capacity = 0
+    cfg.sort_keys = 0
+    cfg.trace_budget = 16
+    r = sb.Renderer(scene, cfg, eems=ex["eems"], cmf=ex["cmf"], bvh_params={"width": 4})
+    B = cfg.bands
+    for k in range(B):
+        r.cast_rays(k, pass_idx=(1 << 26) + k)  # warm-up
+    n = max(1, min(blocks, timed_blocks))
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for b in range(n):
+        for k in range(B):
+            r.cast_rays(k, pass_idx=b * B + k)
+        r.average_and_reset_block(b + 1)
+    e1.record()
+    torch.cuda.synchronize()
+    per_block = e0.elapsed_time(e1) / n * 1e-3
+    bits = r.check_device()
+    r.close()
+    return {"kernel": "depth-synchronous wavefront pass, one launch per pass (four-child nodes)",
+            "seconds_per_block": per_block, "timed_blocks": n, "seconds_same_paths": per_block * blocks,
+            "device_error_bits": bits}
+
+
+def bench_rmse(args):
+    """Seconds to a relative XYZ RMSE target on the single-scene workloads:
+    the batched renderer (the autotuned wavelength bundles) renders blocks
+    until the image's estimated RMSE reaches the target (measured end to end,
+    with the bias check against the FP64 oracle image); the plain single-scene
+    kernel is timed on the same paths.  Prints one JSON line."""
+    rank, world, _ = dist_env()
+    sampler = ClockSampler(gpu_uuid(0))
+    sampler.start()
+    legs = []
+    for name in args.rmse_workloads.split(","):
+        leg = rmse_leg(name, args.rmse_target, args.rmse_seconds, bundles=True)
+        leg["plain"] = plain_seconds(name, leg["blocks"])
+        leg["speedup_vs_plain"] = leg["plain"]["seconds_same_paths"] / leg["seconds"]
+        legs.append(leg)
+    clocks = sampler.stop()
+    print(json.dumps({"metric": f"seconds to {args.rmse_target:.0%} relative XYZ RMSE", "unit": "s",
+                      "higher_is_better": False, "n_gpus": 1, "data": "synthetic (seeded procedural scenes)",
+                      "legs": legs, "clocks": clocks}))
 
 
 def adjoint_leg():
@@ -765,5 +823,7 @@ if __name__ == "__main__":
         bench_batch(a)
     elif a.workload == "adjoint":
         bench_adjoint(a)
+    elif a.workload == "rmse":
+        bench_rmse(a)
     else:
         bench_ours(a)

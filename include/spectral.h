@@ -125,6 +125,15 @@ const char *ts_version(void);
 /* ---- scene (setup_scene + build_bvh + get_scene_dimensions, main.py:398-631) */
 ts_status ts_upload_scene(ts_ctx *ctx, const ts_scene_desc *scene);
 ts_status ts_scene_info_get(const ts_ctx *ctx, ts_scene_info *info);
+
+/* A view of another context's scene (new; the reference renders one camera of
+ * one scene): a context with its own config (resolution, depth, seed, scene id,
+ * launch settings), camera and film that renders the owner's uploaded scene
+ * without uploading or copying it.  Bands and wavelength range must equal the
+ * owner's.  The owner must outlive its views; the material tables are shared
+ * (ts_update_materials through either updates both); ts_upload_scene on a
+ * view gives it a scene of its own.  Views batch like any context. */
+ts_status ts_create_view(const ts_ctx *owner, const ts_config *cfg, ts_ctx **out);
 /* slot -> original triangle index, [num_tris] host array */
 ts_status ts_get_tri_perm(const ts_ctx *ctx, int32_t *perm_out);
 
@@ -275,10 +284,17 @@ ts_status ts_adjoint_passes(ts_ctx *ctx, uint32_t first_pass, int32_t num_passes
  * scene order. */
 typedef struct ts_batch ts_batch;
 typedef struct {
-  int32_t block_size;     /* render-kernel threads per block, 32..128 (0 = 128) */
-  int32_t blocks_per_sm;  /* persistent grid = SMs * blocks_per_sm (0 = 5) */
-  int32_t use_graph;      /* 1: capture the step's four kernels as one CUDA graph at the first step, replay after */
-  int32_t occupancy;      /* 0 = 5 resident blocks per SM (96 registers), 8 = 8 blocks (64 registers) */
+  int32_t block_size;     /* megakernel: threads per block, 32..128 (0 = 128) */
+  int32_t blocks_per_sm;  /* megakernel: persistent grid = SMs * blocks_per_sm (0 = 5) */
+  int32_t use_graph;      /* 1: capture a step as one CUDA graph at the first step, replay it after */
+  int32_t occupancy;      /* megakernel: 0 = 5 resident blocks per SM (96 registers), 8 = 8 blocks (64 registers) */
+  int32_t kernel;         /* TS_KERNEL_MEGA: one persistent megakernel per step; TS_KERNEL_WAVEFRONT: one
+                             regenerating wavefront loop over every active scene's block per step (init kernel,
+                             then a while-loop of trace -> shade over all scenes' paths), the whole step one
+                             CUDA graph with use_graph */
+  int32_t queue_capacity; /* wavefront: path slots shared by all scenes (0 = min(paths per step, 2^24); at most
+                             2^25; 160 B of device memory per slot) */
+  int32_t trace_budget;   /* wavefront: traversal steps between refills of idle lanes (0 = 16) */
 } ts_batch_config;
 
 ts_status ts_batch_create(const ts_batch_config *cfg, ts_ctx *const *ctxs, int32_t num_scenes, ts_batch **out);

@@ -78,6 +78,7 @@ SIGNATURES = [
     ("ts_render_passes", ctypes.c_int, [_VP, ctypes.c_uint32, ctypes.c_int32, ctypes.c_int32, _VP]),
     ("ts_wave_loop_iterations", ctypes.c_int, [_VP, _VP, ctypes.POINTER(ctypes.c_int32)]),
     ("ts_set_loop_iteration_limit", ctypes.c_int, [_VP, ctypes.c_int32]),
+    ("ts_create_view", ctypes.c_int, [_VP, ctypes.POINTER(TsConfig), ctypes.POINTER(_VP)]),
     ("ts_record_paths", ctypes.c_int, [_VP, ctypes.c_uint32, ctypes.c_int32]),
     ("ts_render_pass_counted", ctypes.c_int, [_VP, ctypes.c_uint32, ctypes.c_int32, _VP,
                                               ctypes.POINTER(ctypes.c_uint64)]),

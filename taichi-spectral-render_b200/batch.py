@@ -32,7 +32,8 @@ from .renderer import _stream
 
 class TsBatchConfig(ctypes.Structure):
     _fields_ = [("block_size", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32), ("use_graph", ctypes.c_int32),
-                ("occupancy", ctypes.c_int32)]
+                ("occupancy", ctypes.c_int32), ("kernel", ctypes.c_int32), ("queue_capacity", ctypes.c_int32),
+                ("trace_budget", ctypes.c_int32)]
 
 
 def _check(lib, status, handle):
@@ -44,14 +45,21 @@ def _check(lib, status, handle):
 class Batch:
     """Scenes (Renderer objects on one device, one BVH width) rendered together."""
 
-    def __init__(self, renderers, block_size=0, blocks_per_sm=0, use_graph=True, occupancy=0):
+    def __init__(self, renderers, block_size=0, blocks_per_sm=0, use_graph=True, occupancy=0, kernel="mega",
+                 queue_capacity=0, trace_budget=0):
+        """kernel="mega": one persistent megakernel per step; kernel="wavefront": one
+        regenerating wavefront loop over all scenes' paths per step (queue_capacity
+        path slots shared by the scenes, 0 = min(paths per step, 2^24)); with
+        use_graph a step is one CUDA graph either way."""
         self.renderers = list(renderers)
         for r in self.renderers:
             r.flush()
         self.lib = _lib.load()
         n = len(self.renderers)
         arr = (ctypes.c_void_p * n)(*[r._ctx.value for r in self.renderers])
-        cfg = TsBatchConfig(int(block_size), int(blocks_per_sm), 1 if use_graph else 0, int(occupancy))
+        k = {"mega": _lib.KERNEL_MEGA, "wavefront": _lib.KERNEL_WAVEFRONT}[kernel]
+        cfg = TsBatchConfig(int(block_size), int(blocks_per_sm), 1 if use_graph else 0, int(occupancy), k,
+                            int(queue_capacity), int(trace_budget))
         self._h = ctypes.c_void_p()
         _check(self.lib, self.lib.ts_batch_create(ctypes.byref(cfg), arr, n, ctypes.byref(self._h)), None)
         self.active = np.ones(n, bool)

@@ -442,6 +442,38 @@ ts_status ts_upload_scene(ts_ctx *c, const ts_scene_desc *sd) {
   return ts_set_camera(c, c->cam, c->cam + 3, c->cam + 6);
 }
 
+ts_status ts_create_view(const ts_ctx *owner, const ts_config *cfg, ts_ctx **out) {
+  if (!owner || !cfg || !out) return fail(nullptr, TS_ERR_INVALID_ARG, "ts_create_view: null argument");
+  *out = nullptr;
+  if (!owner->has_scene) return fail(nullptr, TS_ERR_NO_SCENE, "ts_create_view: the owner has no scene uploaded");
+  if (cfg->device != owner->cfg.device)
+    return fail(nullptr, TS_ERR_INVALID_ARG, "ts_create_view: a view lives on its owner's device");
+  if (cfg->bands != owner->cfg.bands || cfg->lambda_min_nm != owner->cfg.lambda_min_nm ||
+      cfg->lambda_max_nm != owner->cfg.lambda_max_nm)
+    return fail(nullptr, TS_ERR_INVALID_ARG, "ts_create_view: a view keeps its owner's spectral bands");
+  ts_ctx *c = nullptr;
+  const ts_status st = ts_create(cfg, &c);
+  if (st != TS_OK) return st;
+  // the owner's device scene, shared: nothing is uploaded or copied, and the
+  // view frees none of it (its scene_allocs stay empty)
+  c->ds = owner->ds;
+  c->d_mat = owner->d_mat;
+  c->d_eem = owner->d_eem;
+  c->d_qy = owner->d_qy;
+  c->d_cdf = owner->d_cdf;
+  c->d_cmf = owner->d_cmf;
+  c->perm = owner->perm;
+  c->info = owner->info;
+  c->has_scene = true;
+  const ts_status cs = ts_set_camera(c, owner->cam, owner->cam + 3, owner->cam + 6);
+  if (cs != TS_OK) {
+    ts_destroy(c);
+    return cs;
+  }
+  *out = c;
+  return TS_OK;
+}
+
 ts_status ts_scene_info_get(const ts_ctx *c, ts_scene_info *info) {
   if (!c || !info) return fail(nullptr, TS_ERR_INVALID_ARG, "ts_scene_info_get: null argument");
   *info = c->info;
@@ -884,6 +916,9 @@ ts_status ts_check_device(ts_ctx *c, uint32_t *bits) {
 }  // extern "C"
 
 // ---------------------------------------------------------------- batches
+static cudaError_t alloc_wave_buffers(ts::WaveBuffers &w, std::vector<void *> &allocs, size_t &bytes, int n,
+                                      bool views);
+
 struct ts_batch {
   int device = 0, n = 0, width = 2;
   ts_batch_config cfg{};
@@ -899,6 +934,12 @@ struct ts_batch {
   cudaStream_t cap = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  // batch loop (cfg.kernel == TS_KERNEL_WAVEFRONT): path state over queue_capacity slots
+  ts::WaveBuffers wave{};
+  std::vector<void *> wave_allocs;
+  size_t wave_bytes = 0;
+  ts::BatchLoopGraph *loop = nullptr;
+  int loop_cap = 0, loop_limit = 0;
   std::string err;
 };
 
@@ -917,6 +958,10 @@ ts_status bfail(ts_batch *b, ts_status s, const std::string &msg) {
   } while (0)
 
 void batch_free(ts_batch *b) {
+  ts::free_batch_loop(b->loop);
+  b->loop = nullptr;
+  for (void *p : b->wave_allocs) cudaFree(p);
+  b->wave_allocs.clear();
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
   if (b->cap) cudaStreamDestroy(b->cap);
@@ -946,6 +991,16 @@ ts_status ts_batch_create(const ts_batch_config *cfg, ts_ctx *const *ctxs, int32
       return bfail(nullptr, TS_ERR_INVALID_ARG,
                    "ts_batch_create: all scenes of a batch need the same BVH width and traversal variant");
   }
+  if (cfg && cfg->kernel != TS_KERNEL_MEGA && cfg->kernel != TS_KERNEL_WAVEFRONT)
+    return bfail(nullptr, TS_ERR_INVALID_ARG, "ts_batch_create: kernel must be TS_KERNEL_MEGA or TS_KERNEL_WAVEFRONT");
+  if (cfg && (cfg->queue_capacity < 0 || cfg->queue_capacity > (1 << 25)))
+    return bfail(nullptr, TS_ERR_INVALID_ARG, "ts_batch_create: queue_capacity must be 0..2^25");
+  {
+    int64_t total = 0;
+    for (int i = 0; i < n; ++i) total += (int64_t)ctxs[i]->cfg.bands * ctxs[i]->cfg.width * ctxs[i]->cfg.height;
+    if (total + (1 << 25) > INT32_MAX)
+      return bfail(nullptr, TS_ERR_CAPACITY, "ts_batch_create: more than 2^31 paths per step");
+  }
   ts_batch *b = new ts_batch();
   b->device = ctxs[0]->cfg.device;
   b->n = n;
@@ -954,6 +1009,8 @@ ts_status ts_batch_create(const ts_batch_config *cfg, ts_ctx *const *ctxs, int32
   if (b->cfg.block_size <= 0) b->cfg.block_size = 128;
   b->cfg.block_size = std::min(128, std::max(32, b->cfg.block_size / 32 * 32));
   if (b->cfg.blocks_per_sm <= 0) b->cfg.blocks_per_sm = 5;  // the render kernel's resident blocks per SM
+  if (b->cfg.kernel == TS_KERNEL_WAVEFRONT && b->cfg.queue_capacity <= 0) b->cfg.queue_capacity = 1 << 24;
+  if (b->cfg.trace_budget <= 0) b->cfg.trace_budget = 16;
   cudaSetDevice(b->device);
   cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, b->device);
   // Work-pool order: deepest scenes first (then larger frames), so that a
@@ -986,6 +1043,22 @@ ts_status ts_batch_create(const ts_batch_config *cfg, ts_ctx *const *ctxs, int32
   if (e == cudaSuccess) e = cudaMemcpy(b->d_active, b->active.data(), sizeof(int) * n, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = ts::batch_set_smem_limit(n);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking);
+  if (e == cudaSuccess && b->cfg.kernel == TS_KERNEL_WAVEFRONT) {
+    // path slots of the loop: the step's work items (all scenes active), at most queue_capacity
+    int64_t total = 0;
+    int depth = 0;
+    for (int k = 0; k < n; ++k) {
+      const ts::DevConfig &c = b->host[k].c;
+      total += (int64_t)c.B * c.W * c.H;
+      depth = std::max(depth, c.max_depth);
+    }
+    const int64_t cap = std::max<int64_t>(1, std::min<int64_t>(total, b->cfg.queue_capacity));
+    // every slot starts a new item at least once per max_depth iterations while items are left
+    const int64_t bound = ((total + cap - 1) / cap + 2) * (int64_t)(depth + 1) + 4;
+    b->loop_cap = (int)cap;
+    b->loop_limit = (int)std::min<int64_t>(bound, INT32_MAX);
+    e = alloc_wave_buffers(b->wave, b->wave_allocs, b->wave_bytes, b->loop_cap, true);
+  }
   if (e != cudaSuccess) {
     const std::string msg = std::string("ts_batch_create: ") + cudaGetErrorString(e);
     batch_free(b);
@@ -1038,6 +1111,16 @@ ts_status ts_batch_step(ts_batch *b, void *stream) {
   cudaSetDevice(b->device);
   const int grid = b->num_sms * b->cfg.blocks_per_sm;
   const int acc_blocks = b->num_sms * 2;
+  if (b->cfg.kernel == TS_KERNEL_WAVEFRONT) {
+    // one regenerating wavefront loop over every active scene's block; with
+    // use_graph the whole step (prepare, init, while-loop, averages) is one graph
+    TS_BCUDA(b, ts::launch_batch_loop_step(b->d_slots, b->n, b->d_hdr, b->d_active, b->d_err, b->wave, b->width,
+                                           b->num_sms * 8, ts::kMaxBlock, b->cfg.trace_budget, b->loop_cap,
+                                           b->loop_limit, acc_blocks, as_stream(stream), &b->loop,
+                                           b->cfg.use_graph != 0),
+             "ts_batch_step");
+    return TS_OK;
+  }
   if (!b->cfg.use_graph) {
     TS_BCUDA(b, ts::launch_batch_step(b->d_slots, b->n, b->d_hdr, b->d_active, b->d_err, b->width, grid,
                                       b->cfg.block_size, acc_blocks, as_stream(stream), b->cfg.occupancy),
@@ -1070,6 +1153,40 @@ ts_status ts_batch_check(ts_batch *b, uint32_t *bits) {
 
 }  // extern "C"
 
+// path-state buffers of the wavefront renderers: n slots (views: also the
+// per-slot and per-query batch view arrays of the batch loop)
+static cudaError_t alloc_wave_buffers(ts::WaveBuffers &w, std::vector<void *> &allocs, size_t &bytes, int n,
+                                      bool views) {
+  auto grab = [&](void **p, size_t b) -> cudaError_t {
+    cudaError_t e = cudaMalloc(p, b);
+    if (e == cudaSuccess) {
+      allocs.push_back(*p);
+      bytes += b;
+    }
+    return e;
+  };
+  const size_t N = (size_t)n;
+  cudaError_t e = cudaSuccess;
+  for (auto *p : {(void **)&w.pos_thr, (void **)&w.dir_spdf, (void **)&w.hit, (void **)&w.sq_origin,
+                  (void **)&w.sq_dir})
+    if (e == cudaSuccess) e = grab(p, N * sizeof(float4));
+  for (auto *p : {(void **)&w.meta, (void **)&w.sq_meta})
+    if (e == cudaSuccess) e = grab(p, N * sizeof(int4));
+  for (auto *p : {(void **)&w.queue[0], (void **)&w.queue[1], (void **)&w.shadow_queue, (void **)&w.sorted,
+                  (void **)&w.trace_order, (void **)&w.shadow_order, (void **)&w.tag})
+    if (e == cudaSuccess) e = grab(p, N * sizeof(int));
+  if (views) {
+    for (auto *p : {(void **)&w.view, (void **)&w.sq_view})
+      if (e == cudaSuccess) e = grab(p, N * sizeof(int));
+  }
+  if (e == cudaSuccess) e = grab((void **)&w.counts, 8192 * sizeof(int));
+  if (e == cudaSuccess) e = grab((void **)&w.key_hist, 2 * ts::kMaxKeys * sizeof(int));
+  if (e == cudaSuccess) e = grab((void **)&w.loop, sizeof(ts::WaveLoop));
+  if (e == cudaSuccess) e = cudaMemset(w.loop, 0, sizeof(ts::WaveLoop));
+  if (e == cudaSuccess) w.capacity = n;
+  return e;
+}
+
 // wavefront buffers are created on first use (one slot per pixel)
 static ts_status ensure_wave(ts_ctx *c) {
   const int npix = c->cfg.width * c->cfg.height;
@@ -1078,34 +1195,6 @@ static ts_status ensure_wave(ts_ctx *c) {
   free_list(c->wave_allocs);
   c->wave = ts::WaveBuffers{};
   c->wave_bytes = 0;
-  auto grab = [&](void **p, size_t bytes) -> cudaError_t {
-    cudaError_t e = cudaMalloc(p, bytes);
-    if (e == cudaSuccess) {
-      c->wave_allocs.push_back(*p);
-      c->wave_bytes += bytes;
-    }
-    return e;
-  };
-  ts::WaveBuffers &w = c->wave;
-  const size_t N = (size_t)n;
-  TS_CUDA(c, grab((void **)&w.pos_thr, N * sizeof(float4)), "wavefront buffers");
-  TS_CUDA(c, grab((void **)&w.dir_spdf, N * sizeof(float4)), "wavefront buffers");
-  TS_CUDA(c, grab((void **)&w.meta, N * sizeof(int4)), "wavefront buffers");
-  TS_CUDA(c, grab((void **)&w.hit, N * sizeof(float4)), "wavefront buffers");
-  TS_CUDA(c, grab((void **)&w.sq_origin, N * sizeof(float4)), "wavefront buffers");
-  TS_CUDA(c, grab((void **)&w.sq_dir, N * sizeof(float4)), "wavefront buffers");
-  TS_CUDA(c, grab((void **)&w.sq_meta, N * sizeof(int4)), "wavefront buffers");
-  TS_CUDA(c, grab((void **)&w.queue[0], N * sizeof(int)), "wavefront buffers");
-  TS_CUDA(c, grab((void **)&w.queue[1], N * sizeof(int)), "wavefront buffers");
-  TS_CUDA(c, grab((void **)&w.shadow_queue, N * sizeof(int)), "wavefront buffers");
-  TS_CUDA(c, grab((void **)&w.sorted, N * sizeof(int)), "wavefront buffers");
-  TS_CUDA(c, grab((void **)&w.trace_order, N * sizeof(int)), "wavefront buffers");
-  TS_CUDA(c, grab((void **)&w.shadow_order, N * sizeof(int)), "wavefront buffers");
-  TS_CUDA(c, grab((void **)&w.counts, 8192 * sizeof(int)), "wavefront buffers");
-  TS_CUDA(c, grab((void **)&w.key_hist, 2 * ts::kMaxKeys * sizeof(int)), "wavefront buffers");
-  TS_CUDA(c, grab((void **)&w.tag, N * sizeof(int)), "wavefront buffers");
-  TS_CUDA(c, grab((void **)&w.loop, sizeof(ts::WaveLoop)), "wavefront buffers");
-  TS_CUDA(c, cudaMemset(w.loop, 0, sizeof(ts::WaveLoop)), "wavefront buffers");
-  w.capacity = n;
+  TS_CUDA(c, alloc_wave_buffers(c->wave, c->wave_allocs, c->wave_bytes, n, false), "wavefront buffers");
   return TS_OK;
 }

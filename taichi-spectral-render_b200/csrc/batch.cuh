@@ -27,7 +27,35 @@ struct BatchHeader {
   int counter;  // persistent-pool counter
 };
 
+// the slot whose work items hold idx: the largest slot whose first item is
+// <= idx (an empty slot shares the next one's start and is skipped)
+__device__ __forceinline__ int batch_find_slot(const BatchSlot *sl, int n, int idx) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (sl[mid].item0 <= idx) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
 size_t batch_smem_bytes(int n);
+// the first and last kernels of a step, on their own (the batch loop captures
+// them around its while-loop): item ranges of the active slots; block
+// averages and pass counters of the slots that rendered
+cudaError_t launch_batch_prepare(BatchSlot *slots, int n, BatchHeader *h, const int *active, cudaStream_t st);
+cudaError_t launch_batch_finish(BatchSlot *slots, int n, int acc_blocks, cudaStream_t st);
+
+// One step of the batch as one regenerating wavefront loop over the work items
+// of every active slot (render_wave.cu): prepare, loop init, the while-loop of
+// trace -> shade -> control, block averages, pass advance.  With use_graph
+// the whole step is one CUDA graph (built at the first step, replayed after);
+// limit bounds the loop's iterations (kErrIterationCap past it).
+struct BatchLoopGraph;
+cudaError_t launch_batch_loop_step(BatchSlot *slots, int n, BatchHeader *h, const int *active, uint32_t *err,
+                                   const WaveBuffers &w, int width, int grid, int block, int budget, int capacity,
+                                   int limit, int acc_blocks, cudaStream_t st, BatchLoopGraph **graph, bool use_graph);
+void free_batch_loop(BatchLoopGraph *g);
 cudaError_t batch_set_smem_limit(int n);
 // one step: prepare (item ranges), render (persistent pool), accumulate, advance
 cudaError_t launch_batch_step(BatchSlot *slots, int n, BatchHeader *h, const int *active, uint32_t *err, int width,

@@ -74,6 +74,10 @@ struct WaveBuffers {
   int *tag;           // regenerating loop: path depth | pass offset << 16, per slot
   WaveLoop *loop;     // regenerating loop state
   int capacity;
+  // batch loop only (nullptr otherwise): the batch slot (scene view) of each
+  // path slot and of each shadow query
+  int *view = nullptr;
+  int *sq_view = nullptr;
 };
 constexpr int kMaxKeys = 256;
 

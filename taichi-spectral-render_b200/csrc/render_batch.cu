@@ -34,17 +34,6 @@ __global__ void k_batch_prepare(BatchSlot *slots, int n, BatchHeader *h, const i
   h->counter = 0;
 }
 
-// the largest slot whose first item is <= idx (empty slots share the next one's start)
-__device__ __forceinline__ int find_slot(const BatchSlot *sh, int n, int idx) {
-  int lo = 0, hi = n - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (sh[mid].item0 <= idx) lo = mid;
-    else hi = mid - 1;
-  }
-  return lo;
-}
-
 template <int W, int kMinBlocks = 5>
 __global__ void __launch_bounds__(128, kMinBlocks) k_render_batch(const BatchSlot *__restrict__ slots, int n,
                                                       BatchHeader *__restrict__ h, uint32_t *__restrict__ err) {
@@ -76,7 +65,7 @@ __global__ void __launch_bounds__(128, kMinBlocks) k_render_batch(const BatchSlo
       if (need) {
         const int idx = base + __popc(m & ((1u << lane) - 1u));
         if (idx < total) {
-          slot = find_slot(sh, n, idx);
+          slot = batch_find_slot(sh, n, idx);
           const BatchSlot &sl = sh[slot];
           const int npix = sl.c.W * sl.c.H;
           const int local = idx - sl.item0;
@@ -143,6 +132,17 @@ cudaError_t launch_batch_step(BatchSlot *slots, int n, BatchHeader *h, const int
   block = block > 128 ? 128 : block;
   if (occupancy >= 8) launch_render_batch<8>(slots, n, h, err, width, grid, block, smem, st);
   else launch_render_batch<5>(slots, n, h, err, width, grid, block, smem, st);
+  k_batch_accumulate<<<dim3(acc_blocks, n), 256, 0, st>>>(slots);
+  k_batch_advance<<<(n + 127) / 128, 128, 0, st>>>(slots, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_prepare(BatchSlot *slots, int n, BatchHeader *h, const int *active, cudaStream_t st) {
+  k_batch_prepare<<<1, 32, 0, st>>>(slots, n, h, active);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_finish(BatchSlot *slots, int n, int acc_blocks, cudaStream_t st) {
   k_batch_accumulate<<<dim3(acc_blocks, n), 256, 0, st>>>(slots);
   k_batch_advance<<<(n + 127) / 128, 128, 0, st>>>(slots, n);
   return cudaGetLastError();

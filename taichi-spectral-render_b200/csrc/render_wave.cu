@@ -21,6 +21,7 @@
 #include <mutex>
 #include <vector>
 
+#include "batch.cuh"
 #include "estimator.cuh"
 #include "kernels.cuh"
 
@@ -353,13 +354,15 @@ __device__ __forceinline__ void shade_path(const DevScene &s, const DevConfig &c
 // Queue appends are bounded by construction (every slot appends at most once
 // per stage); the checks below only keep a corrupted counter from writing
 // past a queue, reporting kErrQueueOverflow instead.
-__device__ __forceinline__ void append_shadow(int *count, const WaveBuffers &w, const Shaded &r, uint32_t *err) {
+__device__ __forceinline__ void append_shadow(int *count, const WaveBuffers &w, const Shaded &r, uint32_t *err,
+                                              int view = -1) {
   const int sslot = warp_append(count, r.nee);
   if (r.nee && sslot >= w.capacity) {
     atomicOr(err, kErrQueueOverflow);
     return;
   }
   if (r.nee) {
+    if (w.sq_view) w.sq_view[sslot] = view;
     w.sq_origin[sslot] = make_float4(r.sq.origin.x, r.sq.origin.y, r.sq.origin.z, r.sq.max_dist);
     w.sq_dir[sslot] = make_float4(r.sq.dir.x, r.sq.dir.y, r.sq.dir.z, r.sq.contrib);
     w.sq_meta[sslot] = make_int4(r.pix, r.sq.light_slot, r.sq.vol, r.sq.band | (r.dep_band << 8));
@@ -688,6 +691,327 @@ cudaError_t launch_wave_loop(const DevScene &s, const DevConfig &c, uint32_t pas
   k_loop_init<<<init_grid, 256, 0, st>>>(s, c, w, w.loop, pass0, band0, npass, n0, limit, shared);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
+  return cudaGraphLaunch(G.exec, st);
+}
+
+// ---------------------------------------------------------------------------
+// The batch loop: many scene views (batch slots, each a context's scene,
+// camera, resolution, depth and film) in one regenerating wavefront loop.
+// The work items of a step are the concatenation of the active slots' items
+// (a whole spectral block of each, k_batch_prepare); a path slot carries the
+// view of its item in w.view and a shadow query in w.sq_view, and every stage
+// reads that view's scene, config and film from the slot table.  Paths are
+// exactly those of ts_render_pass on each view's context: the same random
+// streams (seed, pass, pixel, scene id), the same event functions.
+namespace {
+
+// item -> view, pass offset and pixel of the current step
+struct BatchItem {
+  int view, po, pix;
+};
+__device__ __forceinline__ BatchItem batch_item(const BatchSlot *slots, int n, int item) {
+  BatchItem r;
+  r.view = batch_find_slot(slots, n, item);
+  const BatchSlot &sl = slots[r.view];
+  const int npix = sl.c.W * sl.c.H;
+  const int local = item - sl.item0;
+  r.po = local / npix;
+  r.pix = local - r.po * npix;
+  return r;
+}
+
+__device__ __forceinline__ int slot_band(const BatchSlot &sl, int po) {
+  int b = sl.band0 + po;
+  return b >= sl.c.B ? b - sl.c.B : b;
+}
+
+// deposits share film cells between passes in flight only where fluorescence moves them
+__device__ __forceinline__ bool slot_shared(const BatchSlot &sl) { return sl.s.num_eems > 0; }
+
+__device__ __forceinline__ void start_batch_path(const BatchSlot *slots, int n, const WaveBuffers &w, int item,
+                                                 int q) {
+  const BatchItem it = batch_item(slots, n, item);
+  const BatchSlot &sl = slots[it.view];
+  start_path(sl.s.cam_o, sl.s.cam_u, sl.s.cam_v, sl.s.cam_w, sl.c, sl.pass0 + (uint32_t)it.po, slot_band(sl, it.po),
+             it.pix, w, q);
+  w.tag[q] = it.po << 16;
+  w.view[q] = it.view;
+}
+
+__global__ void k_bloop_init(const BatchSlot *__restrict__ slots, int n, const BatchHeader *__restrict__ h,
+                             WaveBuffers w, WaveLoop *L, int capacity, int limit) {
+  const int total = h->total;
+  const int n0 = total < capacity ? total : capacity;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n0; q += gridDim.x * blockDim.x) {
+    start_batch_path(slots, n, w, q, q);
+    w.queue[0][q] = q;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    L->ext[0] = n0;
+    L->ext[1] = 0;
+    L->sh[0] = L->sh[1] = 0;
+    L->fetch[0] = L->fetch[1] = 0;
+    L->next_item = n0;
+    L->total = total;
+    L->iter = 0;
+    L->limit = limit;
+    L->go = n0 > 0 ? 1 : 0;
+  }
+}
+
+// trace stage of the batch loop: k_trace<W, true> with each item's view
+template <int W>
+__global__ void __launch_bounds__(kMaxBlock, 4) k_trace_bloop(const BatchSlot *__restrict__ slots, WaveBuffers w,
+                                                           uint32_t *__restrict__ err, int budget, WaveLoop *L) {
+  uint32_t eb = 0;
+  const int a = L->iter & 1;
+  const int nsh = L->sh[a ^ 1];
+  const int next = L->ext[a];
+  const int *q = w.queue[a];
+  int *fetch = L->fetch + 0;
+  const int total = nsh + next;
+  const int lane = threadIdx.x & 31;
+  int item = -1, pid = 0, pixel = 0, band = 0, dep_band = 0, v = 0;
+  bool exhausted = false;
+  Traversal t;
+  int2 stack[StackSize<W>::value];
+  ShadowQuery sq;
+  ShadowState ss;
+  for (;;) {
+    const bool need = item < 0 && !exhausted;
+    const unsigned m = __ballot_sync(0xffffffffu, need);
+    if (m) {
+      const int leader = __ffs(m) - 1;
+      int base = 0;
+      if (lane == leader) base = atomicAdd(fetch, __popc(m));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (need) {
+        const int idx = base + __popc(m & ((1u << lane) - 1u));
+        if (idx >= total) {
+          exhausted = true;
+        } else if (idx < nsh) {
+          item = idx;
+          v = w.sq_view[idx];
+          const BatchSlot &sl = slots[v];
+          const float4 o = w.sq_origin[idx], d = w.sq_dir[idx];
+          const int4 mm = w.sq_meta[idx];
+          sq.origin = xyz(o);
+          sq.max_dist = o.w;
+          sq.dir = xyz(d);
+          sq.contrib = d.w;
+          sq.light_slot = mm.y;
+          sq.vol = mm.z;
+          pixel = mm.x;
+          band = mm.w & 0xff;
+          dep_band = mm.w >> 8;
+          ss.pos = sq.origin;
+          ss.total = 1.f;
+          ss.traveled = 0.f;
+          ss.vol = sq.vol;
+          ss.seg = 0;
+          trav_begin(sl.s, t, ss.pos, sq.dir, shadow_bound(sl.s, sl.c, sq, ss, band));
+        } else {
+          item = idx;
+          pid = q[idx - nsh];
+          v = w.view[pid];
+          const float4 pt = w.pos_thr[pid], ds = w.dir_spdf[pid];
+          trav_begin(slots[v].s, t, xyz(pt), xyz(ds), slots[v].c.escape);
+        }
+      }
+    }
+    if (__ballot_sync(0xffffffffu, item >= 0) == 0) break;
+    const BatchSlot &sl = slots[v];
+    if (item >= 0 && trav_advance<W>(sl.s, t, stack, sl.c.eps, budget, eb)) {
+      if (item < nsh) {
+        if (shadow_segment(sl.s, sl.c, sq, t.h, band, ss)) {
+          if (ss.total > 1e-6f) deposit(sl.f, pixel, dep_band, sq.contrib * ss.total, slot_shared(sl));
+          item = -1;
+        } else {
+          trav_begin(sl.s, t, ss.pos, sq.dir, shadow_bound(sl.s, sl.c, sq, ss, band));
+        }
+      } else {
+        w.hit[pid] = make_float4(t.h.t, t.h.u, t.h.v, __int_as_float(t.h.slot));
+        item = -1;
+      }
+    }
+  }
+  if (eb) atomicOr(err, eb);
+}
+
+// shade stage of the batch loop: k_shade_loop with each item's view; an ended
+// path's slot starts the next work item of the whole pool, whichever view it
+// belongs to
+__global__ void __launch_bounds__(kMaxBlock, 4) k_shade_bloop(const BatchSlot *__restrict__ slots, int nslots,
+                                                           WaveBuffers w, WaveLoop *L, uint32_t *err) {
+  const int a = L->iter & 1;
+  const int n = L->ext[a];
+  const int *q = w.queue[a];
+  int *qn = w.queue[a ^ 1];
+  const int total = L->total;
+  const bool more = L->next_item < total;
+  for (;;) {
+    const int base = warp_fetch(L->fetch + 1);
+    if (base >= n) break;
+    const int i = base + (threadIdx.x & 31);
+    Shaded r;
+    r.cont = r.nee = false;
+    r.pix = -1;
+    r.dep_band = 0;
+    int pid = -1, v = 0;
+    if (i < n) {
+      pid = q[i];
+      v = w.view[pid];
+      const BatchSlot &sl = slots[v];
+      const int tag = w.tag[pid];
+      const int po = tag >> 16;
+      shade_path(sl.s, sl.c, sl.pass0 + (uint32_t)po, slot_band(sl, po), (tag & 0xffff) + 1 >= sl.c.max_depth, sl.f,
+                 w, pid, slot_shared(sl), r);
+      if (r.cont) w.tag[pid] = tag + 1;
+    }
+    append_shadow(L->sh + a, w, r, err, v);
+    bool fresh = false;
+    if (more) {
+      const int item = warp_append(&L->next_item, pid >= 0 && !r.cont);
+      if (item >= 0 && item < total) {
+        start_batch_path(slots, nslots, w, item, pid);
+        fresh = true;
+      }
+    }
+    append_ext(L->ext + (a ^ 1), qn, pid, r.cont || fresh, w.capacity, err);
+  }
+}
+
+}  // namespace
+
+struct BatchLoopGraph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t capture = nullptr;
+};
+
+void free_batch_loop(BatchLoopGraph *g) {
+  if (!g) return;
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  if (g->capture) cudaStreamDestroy(g->capture);
+  delete g;
+}
+
+namespace {
+
+cudaError_t launch_trace_bloop(const BatchSlot *slots, const WaveBuffers &w, uint32_t *err, int width, int grid,
+                               int block, int budget, cudaStream_t st) {
+  if (width == 8) k_trace_bloop<8><<<grid, block, 0, st>>>(slots, w, err, budget, w.loop);
+  else if (width == 4) k_trace_bloop<4><<<grid, block, 0, st>>>(slots, w, err, budget, w.loop);
+  else if (width == 3) k_trace_bloop<3><<<grid, block, 0, st>>>(slots, w, err, budget, w.loop);
+  else k_trace_bloop<2><<<grid, block, 0, st>>>(slots, w, err, budget, w.loop);
+  return cudaGetLastError();
+}
+
+// the loop body: one iteration (trace, shade, control)
+cudaError_t bloop_body(BatchSlot *slots, int n, const WaveBuffers &w, uint32_t *err, int width, int grid, int block,
+                       int budget, cudaGraphConditionalHandle h, int in_graph, cudaStream_t st) {
+  cudaError_t e = launch_trace_bloop(slots, w, err, width, grid, block, budget, st);
+  if (e != cudaSuccess) return e;
+  k_shade_bloop<<<grid, block, 0, st>>>(slots, n, w, w.loop, err);
+  k_loop_control<<<1, 32, 0, st>>>(w.loop, h, in_graph, err);
+  return cudaGetLastError();
+}
+
+cudaError_t bloop_head(BatchSlot *slots, int n, BatchHeader *h, const int *active, const WaveBuffers &w, int capacity,
+                       int limit, cudaStream_t st) {
+  cudaError_t e = launch_batch_prepare(slots, n, h, active, st);
+  if (e != cudaSuccess) return e;
+  const int init_grid = (capacity + 255) / 256 < 4096 ? (capacity + 255) / 256 : 4096;
+  k_bloop_init<<<init_grid, 256, 0, st>>>(slots, n, h, w, w.loop, capacity, limit);
+  return cudaGetLastError();
+}
+
+// the whole step as one graph: head -> while(loop body) -> finish
+cudaError_t build_bloop_graph(BatchLoopGraph &G, BatchSlot *slots, int n, BatchHeader *h, const int *active,
+                              uint32_t *err, const WaveBuffers &w, int width, int grid, int block, int budget,
+                              int capacity, int limit, int acc_blocks) {
+  cudaError_t e;
+  if (!G.capture && (e = cudaStreamCreateWithFlags(&G.capture, cudaStreamNonBlocking)) != cudaSuccess) return e;
+  if ((e = cudaGraphCreate(&G.graph, 0)) != cudaSuccess) return e;
+  cudaGraphConditionalHandle cond;
+  if ((e = cudaGraphConditionalHandleCreate(&cond, G.graph, 1, cudaGraphCondAssignDefault)) != cudaSuccess) return e;
+  // head: prepare + init
+  if ((e = cudaStreamBeginCaptureToGraph(G.capture, G.graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)) !=
+      cudaSuccess)
+    return e;
+  cudaError_t le = bloop_head(slots, n, h, active, w, capacity, limit, G.capture);
+  cudaStreamCaptureStatus cs;
+  const cudaGraphNode_t *deps = nullptr;
+  size_t ndeps = 0;
+  std::vector<cudaGraphNode_t> head;
+  if (le == cudaSuccess) le = cudaStreamGetCaptureInfo(G.capture, &cs, nullptr, nullptr, &deps, &ndeps);
+  if (le == cudaSuccess) head.assign(deps, deps + ndeps);
+  cudaGraph_t g2 = nullptr;
+  e = cudaStreamEndCapture(G.capture, &g2);
+  if (le != cudaSuccess) return le;
+  if (e != cudaSuccess) return e;
+  // the while-loop
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = cond;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t loop;
+  if ((e = cudaGraphAddNode(&loop, G.graph, head.data(), head.size(), &cp)) != cudaSuccess) return e;
+  if ((e = cudaStreamBeginCaptureToGraph(G.capture, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                         cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+    return e;
+  le = bloop_body(slots, n, w, err, width, grid, block, budget, cond, 1, G.capture);
+  cudaGraph_t body = nullptr;
+  e = cudaStreamEndCapture(G.capture, &body);
+  if (le != cudaSuccess) return le;
+  if (e != cudaSuccess) return e;
+  // tail: block averages and pass counters
+  if ((e = cudaStreamBeginCaptureToGraph(G.capture, G.graph, &loop, nullptr, 1, cudaStreamCaptureModeThreadLocal)) !=
+      cudaSuccess)
+    return e;
+  le = launch_batch_finish(slots, n, acc_blocks, G.capture);
+  e = cudaStreamEndCapture(G.capture, &g2);
+  if (le != cudaSuccess) return le;
+  if (e != cudaSuccess) return e;
+  return cudaGraphInstantiate(&G.exec, G.graph, 0);
+}
+
+}  // namespace
+
+cudaError_t launch_batch_loop_step(BatchSlot *slots, int n, BatchHeader *h, const int *active, uint32_t *err,
+                                   const WaveBuffers &w, int width, int grid, int block, int budget, int capacity,
+                                   int limit, int acc_blocks, cudaStream_t st, BatchLoopGraph **graph,
+                                   bool use_graph) {
+  if (capacity < 1 || capacity > w.capacity || !w.view || !w.sq_view || !w.tag || !w.loop || limit < 1)
+    return cudaErrorInvalidValue;
+  if (!use_graph) {
+    // the same kernels launched from the host, the loop's continue flag read after each iteration
+    cudaError_t e = bloop_head(slots, n, h, active, w, capacity, limit, st);
+    if (e != cudaSuccess) return e;
+    for (int it = 0; it < limit; ++it) {
+      int go = 0;
+      e = cudaMemcpyAsync(&go, &w.loop->go, sizeof(int), cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+      if (e != cudaSuccess) return e;
+      if (!go) break;
+      e = bloop_body(slots, n, w, err, width, grid, block, budget, 0, 0, st);
+      if (e != cudaSuccess) return e;
+    }
+    return launch_batch_finish(slots, n, acc_blocks, st);
+  }
+  if (!*graph) *graph = new BatchLoopGraph;
+  BatchLoopGraph &G = **graph;
+  if (!G.exec) {
+    const cudaError_t e =
+        build_bloop_graph(G, slots, n, h, active, err, w, width, grid, block, budget, capacity, limit, acc_blocks);
+    if (e != cudaSuccess) {
+      if (G.graph) cudaGraphDestroy(G.graph);
+      G.graph = nullptr;
+      return e;
+    }
+  }
   return cudaGraphLaunch(G.exec, st);
 }
 

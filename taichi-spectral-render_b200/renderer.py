@@ -126,6 +126,33 @@ class Renderer:
         self.cmf_scale = cmf_scale
         self.setup_scene(scene_dict, eems=eems, cmf=cmf, bvh=bvh, bvh_params=bvh_params, exact=exact)
 
+    def view(self, config=None, camera=None):
+        """Another camera on this renderer's scene (ts_create_view): a Renderer with
+        its own config (resolution, depth, seed, scene id, launch settings),
+        camera and film that renders this scene without uploading it again.
+        ``config`` keeps this renderer's bands and wavelength range; ``camera`` is
+        a create_scene() camera dictionary (default: this renderer's camera).
+        This renderer must stay open while the view is used."""
+        import torch
+        self.flush()
+        cfg = config or dataclasses.replace(self.config)
+        v = Renderer.__new__(Renderer)
+        v.config = cfg
+        v.lib = self.lib
+        v._ctx = ctypes.c_void_p()
+        _lib.check(self.lib.ts_create_view(self._ctx, ctypes.byref(cfg.to_c()), ctypes.byref(v._ctx)))
+        v.device = torch.device("cuda", cfg.device)
+        v._pending = []
+        v.total_samples = 0
+        v.num_blocks_completed = 0
+        v._cam = self._cam
+        v.compiled = self.compiled
+        v.cmf_scale = self.cmf_scale
+        v._owner = self
+        if camera is not None:
+            v.update_camera(camera["origin"], camera["lookat"], camera["up"])
+        return v
+
     # ---------------------------------------------------------------- lifecycle
     def close(self):
         self._pending = []

@@ -171,3 +171,62 @@ def test_stream_batch_equals_single_scene_renders():
             assert sbatch.relative_rmse_estimate(r, int(nb)) <= 0.05
     for r in rs:
         r.close()
+
+
+@pytest.mark.parametrize("queue_capacity,use_graph", [(0, True), (3000, True), (3000, False)])
+def test_batch_loop_equals_single_scene_renders(queue_capacity, use_graph):
+    """The batch loop (every scene's block in one regenerating wavefront loop,
+    the step one CUDA graph) gives each scene the films of its own single-pass
+    renders -- with path slots for all items, and with a few thousand slots that
+    the scenes' items regenerate through."""
+    scenes = [make(fn, **kw) for fn, kw in SCENES]
+    refs = [single_scene_mean(a, 2, first_pass=30) for a in scenes]
+    rs = [renderer(a) for a in scenes]
+    try:
+        with sbatch.Batch(rs, kernel="wavefront", queue_capacity=queue_capacity, use_graph=use_graph) as b:
+            b.reset(first_pass=30)
+            b.step()
+            b.step()
+            assert b.check() == 0
+            for r, (mean, m2) in zip(rs, refs):
+                assert same_film(r.mean_film, mean) and same_film(r.m2_film, m2)
+            # inactive scenes keep their films; the others go on
+            before = [r.mean_film.clone() for r in rs]
+            b.set_active([1, 0, 1])
+            b.step()
+            assert b.check() == 0
+            assert torch.equal(rs[1].mean_film, before[1])
+            assert not torch.equal(rs[0].mean_film, before[0])
+    finally:
+        for r in rs:
+            r.close()
+
+
+def test_views_share_one_scene_and_batch_together():
+    """A view renders the owner's scene through its own camera, resolution and
+    film without a second upload: the same film as a separate context holding
+    the same scene and camera, alone and in a batch loop with its owner."""
+    import dataclasses
+    args = make(configs.box_scene, width=32, height=24, depth=5)
+    s, c, ex, bvh = args
+    cam2 = {"origin": [0.2, 0.1, 0.45], "lookat": [0.0, -0.1, -0.5], "up": [0.0, 1.0, 0.0]}
+    c2 = dataclasses.replace(c, width=40, height=30, seed=5, scene_id=3)
+    ref_owner = single_scene_mean(args, 1, first_pass=10)
+    ref_view = single_scene_mean((dict(s, camera=cam2), c2, ex, bvh), 1, first_pass=10)
+    with renderer(args) as r:
+        v = r.view(c2, camera=cam2)
+        try:
+            assert v.scene_info()["device_bytes"] < r.scene_info()["device_bytes"]
+            B = c.bands
+            for k in range(B):
+                v.cast_rays(k, pass_idx=10 + k)
+            v.average_and_reset_block(1)
+            assert same_film(v.mean_film, ref_view[0])
+            for kernel in ("wavefront", "mega"):
+                with sbatch.Batch([r, v], kernel=kernel) as b:
+                    b.reset(first_pass=10)
+                    b.step()
+                    assert b.check() == 0
+                    assert same_film(r.mean_film, ref_owner[0]) and same_film(v.mean_film, ref_view[0])
+        finally:
+            v.close()

@@ -120,7 +120,7 @@ def _first_of_each_kind():
     return [seen[k] for k in ("box", "terrain", "volume")]
 
 
-@pytest.mark.parametrize("engine", ["kernel", "streams"])
+@pytest.mark.parametrize("engine", ["kernel", "loop", "streams"])
 def test_batched_scenes_of_every_kind_match_oracle(engine):
     scenes = _first_of_each_kind()
     rs, oracles = [], []
@@ -134,7 +134,10 @@ def test_batched_scenes_of_every_kind_match_oracle(engine):
     try:
         B = rs[0].config.bands
         first = 300
-        with (sbatch.Batch(rs, use_graph=True) if engine == "kernel" else sbatch.StreamBatch(rs, streams=4)) as b:
+        eng = (sbatch.Batch(rs, use_graph=True) if engine == "kernel" else
+               sbatch.Batch(rs, use_graph=True, kernel="wavefront") if engine == "loop" else
+               sbatch.StreamBatch(rs, streams=4))
+        with eng as b:
             b.reset(first_pass=first)
             b.step()  # one block of every scene, then its block average (n = 1)
             assert b.check() == 0
