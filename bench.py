@@ -31,6 +31,7 @@ sys.path.insert(0, ROOT)
 
 # algorithmic bytes of one unit of work, for the roofline (layouts in csrc/common.cuh)
 BYTES_NODE = 64      # one two-child BVH node (two child boxes + links); wide nodes 128 / 256 B
+BYTES_NODE_Q = {4: 64, 8: 96}  # quantized wide nodes (origin, scales, links, 8-bit child boxes)
 BYTES_TRI = 48       # one triangle test (v0, e1, e2 as float4)
 BYTES_HIT = 48       # shading normals of a resolved hit (3 float4)
 BYTES_MAT_VERTEX = 8 * 32  # material lookups per path vertex (8 x two float4)
@@ -46,6 +47,7 @@ def parse():
     p.add_argument("--kernel", default="mega", choices=["mega", "wavefront"])
     p.add_argument("--workload", default="terrain", choices=["terrain", "box", "volume", "batch", "adjoint", "rmse"])
     p.add_argument("--width", type=int, default=2, choices=[2, 4, 8], help="BVH node width")
+    p.add_argument("--quantize", action="store_true", help="4- / 8-wide nodes with 8-bit child boxes (--no-tune)")
     p.add_argument("--traversal", default="default", choices=["default", "speculative"])
     p.add_argument("--occupancy", type=int, default=0, choices=[0, 8], help="megakernel register budget (--no-tune)")
     p.add_argument("--launch", default="bundle", choices=["bundle", "pass"],
@@ -245,7 +247,7 @@ def rmse_leg(name, target, seconds, bundles=True):
     best, _ = autotune.tune(scene, cfg, eems=ex["eems"], cmf=ex["cmf"], candidates=cands, passes=50 if bundles else 6,
                             first_pass=1 << 26, bundles=bundles)
     cfg = best.apply(cfg)
-    r = sb.Renderer(scene, cfg, eems=ex["eems"], cmf=ex["cmf"], bvh_params={"width": best.width})
+    r = sb.Renderer(scene, cfg, eems=ex["eems"], cmf=ex["cmf"], bvh_params=best.bvh_params())
     B = cfg.bands
     r.cast_rays_bundle(0, B, pass_idx=0)
     r.clear_pixel_space()
@@ -273,7 +275,7 @@ def rmse_leg(name, target, seconds, bundles=True):
     secs = time.perf_counter() - t0
     est = sbatch.relative_rmse_estimate(r, nb)
     out = {"workload": name, "target": target, "blocks": nb, "spp": nb * B, "seconds": secs,
-           "launch": {"kernel": best.kernel, "width": best.width, "traversal": best.traversal,
+           "launch": {"kernel": best.kernel, "width": best.width, "quantize": best.quantize, "traversal": best.traversal,
                       "block_size": best.block_size, "blocks_per_sm": best.blocks_per_sm,
                       "occupancy": best.occupancy, "queue_capacity": best.queue_capacity,
                       "trace_budget": best.trace_budget},
@@ -500,6 +502,15 @@ def bench_batch(args):
         blocks, tb = b.render_to_rmse(target=target)
         bits = b.check()
     paths = sum(int(n) * B * r.config.width * r.config.height for n, r in zip(blocks, rs))
+    # the same scenes through the batch loop: every scene's block in one regenerating
+    # wavefront loop per step, the step one CUDA graph
+    with sbatch.Batch(rs, kernel="wavefront", use_graph=True) as bl:
+        bl.reset()
+        bl.step()
+        bl.reset()
+        blocks_l, tl = bl.render_to_rmse(target=target)
+        bits |= bl.check()
+    paths_l = sum(int(n) * B * r.config.width * r.config.height for n, r in zip(blocks_l, rs))
     # the same scenes through the stream engine: each scene's block one regenerating
     # wavefront loop launch, the scenes spread over a pool of streams
     with sbatch.StreamBatch(rs, streams=8) as sbt:
@@ -509,13 +520,17 @@ def bench_batch(args):
         blocks_s, ts = sbt.render_to_rmse(target=target)
         bits |= sbt.check()
     paths_s = sum(int(n) * B * r.config.width * r.config.height for n, r in zip(blocks_s, rs))
-    best = "streams" if ts < tb else "kernel"
-    line = {"metric": f"seconds to {target:.0%} relative XYZ RMSE, all scenes", "value": min(tb, ts), "unit": "s",
+    engines = {"kernel": tb, "loop": tl, "streams": ts}
+    best = min(engines, key=engines.get)
+    line = {"metric": f"seconds to {target:.0%} relative XYZ RMSE, all scenes", "value": engines[best], "unit": "s",
             "higher_is_better": False, "n_gpus": 1, "impl": "ours", "data": "synthetic (seeded procedural scenes)",
             "config": {"workload": f"{len(rs)} scenes of seeds 100-{99 + len(rs)}: box / terrain / volume, "
                                    "1k-500k triangles, 128^2-512^2, depth 4-16",
                        "scene_build_seconds": build_s},
-            "plain_seconds": tp, "batched_seconds": min(tb, ts), "speedup": tp / min(tb, ts), "engine": best,
+            "plain_seconds": tp, "batched_seconds": engines[best], "speedup": tp / engines[best], "engine": best,
+            "loop_engine": {"seconds": tl, "speedup": tp / tl, "mpaths_per_s": paths_l / tl / 1e6,
+                            "blocks": [int(x) for x in blocks_l],
+                            "what": "all scenes in one regenerating wavefront loop per step (one CUDA graph)"},
             "kernel_engine": {"seconds": tb, "speedup": tp / tb, "mpaths_per_s": paths / tb / 1e6,
                               "what": "all scenes in one persistent megakernel launch per step (CUDA graph)"},
             "stream_engine": {"seconds": ts, "speedup": tp / ts, "mpaths_per_s": paths_s / ts / 1e6,
@@ -622,17 +637,20 @@ def bench_ours(args):
                                     passes=50 if bundles else 6, first_pass=1 << 26, bundles=bundles)
         cfg = best.apply(cfg)
         args.width, args.kernel, args.traversal, args.occupancy = best.width, best.kernel, best.traversal, best.occupancy
+        args.quantize = best.quantize
         tuned = {"seconds": time.time() - t0, "candidates": len(table),
-                 "best": {"width": best.width, "traversal": best.traversal, "kernel": best.kernel,
+                 "best": {"width": best.width, "quantize": best.quantize, "traversal": best.traversal,
+                          "kernel": best.kernel,
                           "block_size": best.block_size, "blocks_per_sm": best.blocks_per_sm,
                           "occupancy": best.occupancy, "queue_capacity": best.queue_capacity,
                           "trace_budget": best.trace_budget},
-                 "ms_per_pass": {f"w{c.width}/{c.traversal}/{c.kernel}/b{c.block_size}/s{c.blocks_per_sm}"
+                 "ms_per_pass": {f"w{c.width}{'q' if c.quantize else ''}/{c.traversal}/{c.kernel}/b{c.block_size}/s{c.blocks_per_sm}"
                                  f"/o{c.occupancy}/q{c.queue_capacity}/t{c.trace_budget}": round(ms, 4)
                                  for c, ms in table}}
     comp = sb.compile_scene(scene, cfg.bands, eems=ex["eems"], cmf=ex["cmf"])
     bvh = sb._lib.build_bvh_host(comp.tris["v0"], comp.tris["v1"], comp.tris["v2"])
-    r = sb.Renderer(scene, cfg, eems=ex["eems"], cmf=ex["cmf"], bvh=bvh, bvh_params={"width": args.width})
+    r = sb.Renderer(scene, cfg, eems=ex["eems"], cmf=ex["cmf"], bvh=bvh,
+                    bvh_params={"width": args.width, "quantize": args.quantize})
     B = cfg.bands
     npix = cfg.width * cfg.height
     paths_per_step = B * npix  # one step = one spectral block of B passes
@@ -654,7 +672,9 @@ def bench_ours(args):
         step(w, base_pass)
     work = r.cast_rays_counted(12, pass_idx=base_pass + 1)
     torch.cuda.synchronize()
-    node_bytes = BYTES_NODE * (args.width // 2)  # 2 -> 64 B, 4 -> 128 B, 8 -> 256 B
+    info = r.scene_info()
+    node_bytes = (BYTES_NODE_Q[info["node_width"]] if info["node_quantized"]
+                  else BYTES_NODE * (info["node_width"] // 2))  # 2 -> 64 B, 4 -> 128 B, 8 -> 256 B
     bytes_per_path = (node_bytes * work["node_visits"] + BYTES_TRI * work["tri_tests"] + BYTES_HIT * work["hits"]
                       + BYTES_MAT_VERTEX * work["vertices"] + BYTES_DEPOSIT * work["deposits"]) / work["paths"]
 
@@ -735,8 +755,8 @@ def bench_ours(args):
     peak, peak_src = measured_peak()
     step_s = ms_max * 1e-3 / args.steps
     achieved = bytes_per_path * paths_per_step / step_s / 1e9
-    traffic = profiled_traffic(args.kernel, args.workload, args.width, 0 if wave_loop else args.occupancy,
-                               use_bundles)
+    traffic = profiled_traffic(args.kernel, args.workload, f"{args.width}q" if args.quantize else args.width,
+                               0 if wave_loop else args.occupancy, use_bundles)
     kernel_name = ("k_render_mega" if args.kernel == "mega" else
                    "regenerating wavefront loop (k_trace + k_shade_loop + k_loop_control per iteration)"
                    if wave_loop else "depth-synchronous wavefront pass")
@@ -746,7 +766,8 @@ def bench_ours(args):
             "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded procedural scene; no dataset)",
             "config": step_config(cfg, ex, desc, world, comp.num_tris),
-            "launch": {"kernel": args.kernel, "bvh_width": args.width, "traversal": args.traversal,
+            "launch": {"kernel": args.kernel, "bvh_width": args.width, "bvh_quantized": bool(args.quantize),
+                       "node_bytes": node_bytes, "traversal": args.traversal,
                        "occupancy": args.occupancy, "queue_capacity": cfg.queue_capacity,
                        "block_size": cfg.block_size, "trace_budget": cfg.trace_budget, "launches": launches},
             "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": 36,

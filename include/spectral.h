@@ -101,6 +101,9 @@ typedef struct {
   int32_t bvh_bins, bvh_leaf_max;
   float bvh_cost_trav, bvh_cost_tri;
   int32_t bvh_width;                /* device node width 2, 4 or 8 (0 = library default) */
+  int32_t bvh_quantized;            /* 4- and 8-wide nodes: nonzero stores each child box as 8-bit offsets from the
+                                       node's origin, rounded outwards (64 / 96 B per node instead of 128 / 256 B;
+                                       the boxes only grow, so closest hits are unchanged) */
 } ts_scene_desc;
 
 typedef struct {
@@ -109,6 +112,7 @@ typedef struct {
   int32_t max_lights;
   size_t device_bytes;  /* device memory held by the context */
   int32_t node_width;   /* node width of the uploaded device BVH */
+  int32_t node_quantized; /* its child boxes are quantized (ts_scene_desc.bvh_quantized) */
 } ts_scene_info;
 
 /* ---- context (replaces ti.init + the module-global fields, main.py:9, 361-394) */

@@ -50,13 +50,15 @@ class TsSceneDesc(ctypes.Structure):
                 ("node_left", I32P), ("node_right", I32P), ("node_num_tris", I32P), ("node_tri_start", I32P),
                 ("tri_perm", I32P),
                 ("bvh_bins", ctypes.c_int32), ("bvh_leaf_max", ctypes.c_int32),
-                ("bvh_cost_trav", ctypes.c_float), ("bvh_cost_tri", ctypes.c_float), ("bvh_width", ctypes.c_int32)]
+                ("bvh_cost_trav", ctypes.c_float), ("bvh_cost_tri", ctypes.c_float), ("bvh_width", ctypes.c_int32),
+                ("bvh_quantized", ctypes.c_int32)]
 
 
 class TsSceneInfo(ctypes.Structure):
     _fields_ = [("num_tris", ctypes.c_int32), ("num_nodes", ctypes.c_int32), ("num_ref_nodes", ctypes.c_int32),
                 ("max_depth", ctypes.c_int32), ("leaves", ctypes.c_int32), ("sah_cost", ctypes.c_double),
-                ("max_lights", ctypes.c_int32), ("device_bytes", ctypes.c_size_t), ("node_width", ctypes.c_int32)]
+                ("max_lights", ctypes.c_int32), ("device_bytes", ctypes.c_size_t), ("node_width", ctypes.c_int32),
+                ("node_quantized", ctypes.c_int32)]
 
 
 # (name, restype, argtypes) of every entry point declared in include/spectral.h

@@ -4,8 +4,9 @@ Every candidate renders exactly the same paths (the random streams depend
 only on seed, pass, pixel and draw index), so tuning never changes an image,
 only its cost.  Knobs:
 
-  * BVH node width 2 / 4 / 8 (the scene is re-uploaded per width; the host
-    builder's tree is reused),
+  * BVH node width 2 / 4 / 8, and for 4 / 8 full-precision or quantized
+    child boxes (the scene is re-uploaded per layout; the host builder's tree
+    is reused),
   * traversal loop of two-child nodes (default if-if / speculative while-while),
   * kernel: the persistent megakernel or the wavefront stages, and for the
     wavefront its queue sorting (sort_keys bit mask), the traversal steps
@@ -20,7 +21,7 @@ current stream); the fastest wins.  Results are cached in a JSON file keyed by
 a signature of the scene (triangles, materials, resolution, depth, bands).
 
     best, table = tune(scene, cfg, eems=ex["eems"], cmf=ex["cmf"], cache="tune.json")
-    r = Renderer(scene, best.apply(cfg), eems=..., cmf=..., bvh_params={"width": best.width})
+    r = Renderer(scene, best.apply(cfg), eems=..., cmf=..., bvh_params=best.bvh_params())
 """
 import dataclasses
 import hashlib
@@ -46,6 +47,10 @@ class Candidate:
     trace_budget: int = 0
     occupancy: int = 0
     queue_capacity: int = 0
+    quantize: bool = False  # 4- / 8-wide nodes with 8-bit child boxes (64 / 96 B)
+
+    def bvh_params(self):
+        return {"width": self.width, "quantize": self.quantize}
 
     def apply(self, cfg):
         """A copy of cfg with this candidate's launch settings."""
@@ -58,6 +63,7 @@ class Candidate:
 def default_candidates(quick=False):
     out = [Candidate(w, "default", "mega", bs, bpsm) for w in (2, 4, 8) for bs in (64, 128) for bpsm in (0, 5)]
     out += [Candidate(w, "default", "mega", 128, 0, occupancy=8) for w in (2, 4, 8)]
+    out += [Candidate(w, "default", "mega", 128, 0, occupancy=o, quantize=True) for w in (4, 8) for o in (0, 8)]
     out += [Candidate(2, "speculative", "mega", 128, 0), Candidate(2, "speculative", "mega", 128, 0, occupancy=8)]
     if not quick:
         out += [Candidate(w, "default", "wavefront", 128, 0, sk, tb)
@@ -68,15 +74,17 @@ def default_candidates(quick=False):
 MAX_QUEUE_CAPACITY = 1 << 25
 
 
-def bundle_wavefront_candidates(npix, bands, widths=(2, 4), multiples=(2, 4, 8, 16, 32), budgets=(16, 8)):
+def bundle_wavefront_candidates(npix, bands, widths=(2, 4, (4, True), (8, True)), multiples=(2, 4, 8, 16, 32),
+                                budgets=(16, 8)):
     """Regenerating-loop wavefront candidates for wavelength bundles: queue
     capacities of several frames' worth of path slots (passes in flight),
     up to the whole bundle, and traversal steps between lane refills (8 is
     faster on shallow BVHs and deep volume paths, 16 on the 2.6M-triangle
     terrain)."""
     caps = sorted({min(m * npix, bands * npix, MAX_QUEUE_CAPACITY) for m in multiples})
-    return [Candidate(w, "default", "wavefront", 256, 0, 0, tb, queue_capacity=qc)
-            for w in widths for qc in caps for tb in budgets]
+    lay = [w if isinstance(w, tuple) else (w, False) for w in widths]
+    return [Candidate(w, "default", "wavefront", 256, 0, 0, tb, queue_capacity=qc, quantize=q)
+            for w, q in lay for qc in caps for tb in budgets]
 
 
 def signature(compiled, cfg, bundles=False):
@@ -138,10 +146,10 @@ def tune(scene_dict, cfg, eems=None, cmf=None, candidates=None, passes=6, warmup
         extra = bundle_wavefront_candidates(cfg.width * cfg.height, cfg.bands)
         candidates += [c for c in extra if c not in candidates]
     table = []
-    for width in sorted({c.width for c in candidates}):
-        group = [c for c in candidates if c.width == width]
+    for layout in sorted({(c.width, c.quantize) for c in candidates}):
+        group = [c for c in candidates if (c.width, c.quantize) == layout]
         with Renderer(scene_dict, group[0].apply(cfg), eems=eems, cmf=cmf, bvh=bvh,
-                      bvh_params={"width": width}) as r:
+                      bvh_params=group[0].bvh_params()) as r:
             for cand in group:
                 r.set_launch_config(kernel=cand.kernel, traversal=cand.traversal, block_size=cand.block_size,
                                     blocks_per_sm=cand.blocks_per_sm, sort_keys=cand.sort_keys,

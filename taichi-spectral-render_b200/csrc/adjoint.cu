@@ -423,7 +423,11 @@ cudaError_t launch_adjoint(const DevScene &s, const DevConfig &c, uint32_t pass,
   if (e != cudaSuccess) return e;
   const int pmat = s.num_materials * 6 * c.B;
   const int psh = adjoint_shared_params(pmat);
-  if (s.node_width == 8) launch_pair<8>(s, c, pass, npass, band, adj, grad, weight, psh, pmat, counter, err, grid, st, rec);
+  if (s.node_width == 9) launch_pair<9>(s, c, pass, npass, band, adj, grad, weight, psh, pmat, counter, err, grid, st, rec);
+  else if (s.node_width == 5)
+    launch_pair<5>(s, c, pass, npass, band, adj, grad, weight, psh, pmat, counter, err, grid, st, rec);
+  else if (s.node_width == 8)
+    launch_pair<8>(s, c, pass, npass, band, adj, grad, weight, psh, pmat, counter, err, grid, st, rec);
   else if (s.node_width == 4)
     launch_pair<4>(s, c, pass, npass, band, adj, grad, weight, psh, pmat, counter, err, grid, st, rec);
   else if (c.speculative)

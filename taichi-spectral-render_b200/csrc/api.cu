@@ -285,7 +285,7 @@ ts_status ts_upload_scene(ts_ctx *c, const ts_scene_desc *sd) {
       return fail(c, TS_ERR_INVALID_ARG, "ts_upload_scene: incomplete reference BVH");
     if (!ts::bvh_from_reference(T, sd->v0, sd->v1, sd->v2, sd->bvh_num_nodes, sd->node_min, sd->node_max,
                                 sd->node_left, sd->node_right, sd->node_num_tris, sd->node_tri_start, sd->tri_perm,
-                                bvh, err, sd->bvh_width > 0 ? sd->bvh_width : kDefaultWidth))
+                                bvh, err, sd->bvh_width > 0 ? sd->bvh_width : kDefaultWidth, sd->bvh_quantized != 0))
       return fail(c, TS_ERR_INVALID_ARG, "ts_upload_scene: " + err);
   } else {
     ts::BvhParams p;
@@ -294,6 +294,7 @@ ts_status ts_upload_scene(ts_ctx *c, const ts_scene_desc *sd) {
     if (sd->bvh_cost_trav > 0) p.cost_trav = sd->bvh_cost_trav;
     if (sd->bvh_cost_tri > 0) p.cost_tri = sd->bvh_cost_tri;
     p.width = sd->bvh_width > 0 ? sd->bvh_width : kDefaultWidth;
+    p.quantize = sd->bvh_quantized != 0;
     if (!ts::build_bvh_binned(T, sd->v0, sd->v1, sd->v2, p, bvh, err))
       return fail(c, TS_ERR_INVALID_ARG, "ts_upload_scene: " + err);
   }
@@ -403,8 +404,8 @@ ts_status ts_upload_scene(ts_ctx *c, const ts_scene_desc *sd) {
   ds.node = d_node;
   ds.tri = d_tri;
   ds.shade = d_shade;
-  ds.node_width = bvh.width;
-  ds.num_nodes = (int)(bvh.node2.size() / ts::node_float4s(bvh.width));
+  ds.node_width = ts::layout_id(bvh.width, bvh.quantized);  // selects the traversal instantiation
+  ds.num_nodes = (int)(bvh.node2.size() / ts::node_float4s(bvh.width, bvh.quantized));
   ds.num_tris = T;
   ds.ref_min = d_rmin;
   ds.ref_max = d_rmax;
@@ -437,6 +438,7 @@ ts_status ts_upload_scene(ts_ctx *c, const ts_scene_desc *sd) {
   c->info.sah_cost = bvh.sah_cost;
   c->info.max_lights = L;
   c->info.node_width = bvh.width;
+  c->info.node_quantized = bvh.quantized ? 1 : 0;
   c->has_scene = true;
   // keep the current camera basis
   return ts_set_camera(c, c->cam, c->cam + 3, c->cam + 6);

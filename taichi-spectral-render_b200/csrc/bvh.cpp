@@ -245,7 +245,67 @@ void expand_big_leaves(std::vector<BNode> &tree, const std::vector<Prim> &prims,
 //   width 8: each of the six rows and the refs as two float4 (16 float4, 256 B)
 // Empty child slots have NaN boxes, which no slab test accepts.  Returns false
 // (out untouched) if the traversal stack bound would be exceeded.
-bool flatten_wide(const std::vector<BNode> &tree, int W, BvhOut &out) {
+// Quantized wide node (layout ids 5 and 9): the node's origin (the low corner
+// of its children's union) and one power-of-two scale per axis; each child
+// box as bytes q with bound = origin + q * scale, rounded outwards so that the
+// decoded box -- computed on the device as one float multiply (exact: q < 256
+// times a power of two) and one float add -- contains the exact box:
+//   float4 0: origin.xyz, (biased scale exponents x, y, z, child count) as bytes
+//   W/4 float4: child refs
+//   then the bytes lo.x[W] hi.x[W] lo.y[W] hi.y[W] lo.z[W] hi.z[W] (4-wide: 24 B + 8 B pad)
+// Returns false if a box cannot be covered (the caller keeps full precision).
+static float q_decode(float origin, int q, float scale) { return origin + (float)q * scale; }
+
+static bool quantize_node(const std::vector<BNode> &tree, const int *ch, int n, const int *ref, int W,
+                          float4 *dst) {
+  float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (int k = 0; k < n; ++k)
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = std::min(lo[a], tree[ch[k]].lo[a]);
+      hi[a] = std::max(hi[a], tree[ch[k]].hi[a]);
+    }
+  float scale[3];
+  int ebias[3];
+  for (int a = 0; a < 3; ++a) {
+    const double ext = (double)hi[a] - (double)lo[a];
+    int e = -126;
+    while (e < 127 && std::ldexp(254.0, e) < ext) ++e;  // extent within 254 steps: one step of margin
+    scale[a] = std::ldexp(1.0f, e);
+    ebias[a] = e + 127;
+  }
+  unsigned char qb[6][8];
+  std::memset(qb, 0, sizeof qb);
+  for (int k = 0; k < n; ++k) {
+    const BNode &c = tree[ch[k]];
+    for (int a = 0; a < 3; ++a) {
+      double ql = std::floor(((double)c.lo[a] - (double)lo[a]) / scale[a]);
+      double qh = std::ceil(((double)c.hi[a] - (double)lo[a]) / scale[a]);
+      int il = (int)std::max(0.0, std::min(255.0, ql)), ih = (int)std::max(0.0, std::min(255.0, qh));
+      while (il > 0 && q_decode(lo[a], il, scale[a]) > c.lo[a]) --il;
+      while (ih < 255 && q_decode(lo[a], ih, scale[a]) < c.hi[a]) ++ih;
+      if (q_decode(lo[a], il, scale[a]) > c.lo[a] || q_decode(lo[a], ih, scale[a]) < c.hi[a]) return false;
+      qb[2 * a][k] = (unsigned char)il;
+      qb[2 * a + 1][k] = (unsigned char)ih;
+    }
+  }
+  uint32_t meta = (uint32_t)ebias[0] | (uint32_t)ebias[1] << 8 | (uint32_t)ebias[2] << 16 | (uint32_t)n << 24;
+  float mf;
+  std::memcpy(&mf, &meta, 4);
+  dst[0] = make_float4(lo[0], lo[1], lo[2], mf);
+  const int per = W / 4;
+  for (int q = 0; q < per; ++q) {
+    int4 l = make_int4(ref[4 * q], ref[4 * q + 1], ref[4 * q + 2], ref[4 * q + 3]);
+    std::memcpy(&dst[1 + q], &l, sizeof(int4));
+  }
+  unsigned char bytes[48];
+  std::memset(bytes, 0, sizeof bytes);
+  for (int r = 0; r < 6; ++r)
+    for (int k = 0; k < W; ++k) bytes[r * W + k] = qb[r][k];
+  std::memcpy(&dst[1 + per], bytes, (size_t)(W == 8 ? 48 : 32));
+  return true;
+}
+
+bool flatten_wide(const std::vector<BNode> &tree, int W, BvhOut &out, bool quantize = false) {
   struct WN {
     int ch[8];
     int n;
@@ -298,6 +358,24 @@ bool flatten_wide(const std::vector<BNode> &tree, int W, BvhOut &out) {
       if (tree[ch[k]].left >= 0) todo.push_back({ch[k], need});
   }
   if (max_stack > kWideStack) return false;
+  if (quantize) {
+    const int F = node_float4s(W, true);
+    std::vector<float4> nodes((size_t)F * wn.size());
+    for (size_t i = 0; i < wn.size(); ++i) {
+      int ref[8];
+      for (int k = 0; k < 8; ++k) ref[k] = leaf_code(0, 1);
+      for (int k = 0; k < wn[i].n; ++k) {
+        const BNode &c = tree[wn[i].ch[k]];
+        ref[k] = c.left >= 0 ? wmap[wn[i].ch[k]] : leaf_code(c.first, c.count);
+      }
+      if (!quantize_node(tree, wn[i].ch, wn[i].n, ref, W, nodes.data() + (size_t)F * i)) return false;
+    }
+    out.node2.swap(nodes);
+    out.width = W;
+    out.quantized = true;
+    out.stack_need = max_stack;
+    return true;
+  }
   const int F = node_float4s(W);
   std::vector<float4> nodes((size_t)F * wn.size());
   const float qnan = std::nanf("");
@@ -333,7 +411,7 @@ bool flatten_wide(const std::vector<BNode> &tree, int W, BvhOut &out) {
 // Flatten a preorder BNode tree into the device layout (two-child, or wide
 // with `width` 4 or 8).  Returns false on a malformed tree.
 bool flatten_two_child(std::vector<BNode> tree, const std::vector<Prim> &prims, const std::vector<int32_t> &perm,
-                       BvhOut &out, std::string &err, int width = 2) {
+                       BvhOut &out, std::string &err, int width = 2, bool quantize = false) {
   expand_big_leaves(tree, prims, perm);
   const int N = (int)tree.size();
   if (N == 0) {
@@ -402,7 +480,9 @@ bool flatten_two_child(std::vector<BNode> tree, const std::vector<Prim> &prims, 
   out.leaves = leaves;
   out.width = 2;
   out.stack_need = maxd;
-  if (width == 4 || width == 8) flatten_wide(tree, width, out);  // keeps the two-child layout if it cannot
+  // keeps the two-child layout if the wide one cannot be built
+  if (width == 4 || width == 8)
+    if (!flatten_wide(tree, width, out, quantize) && quantize) flatten_wide(tree, width, out, false);
   return true;
 }
 
@@ -461,12 +541,13 @@ bool build_bvh_binned(int T, const float *v0, const float *v1, const float *v2, 
     }
   }
   out.sah_cost = cost;
-  return flatten_two_child(std::move(tree), prims, out.perm, out, err, p.width);
+  return flatten_two_child(std::move(tree), prims, out.perm, out, err, p.width, p.quantize);
 }
 
 bool bvh_from_reference(int T, const float *v0, const float *v1, const float *v2, int N, const float *nmin,
                         const float *nmax, const int32_t *left, const int32_t *right, const int32_t *ntris,
-                        const int32_t *tstart, const int32_t *perm, BvhOut &out, std::string &err, int width) {
+                        const int32_t *tstart, const int32_t *perm, BvhOut &out, std::string &err, int width,
+                        bool quantize) {
   out = BvhOut{};
   if (T < 0 || T >= (1 << 27) || N < 0 || (T > 0 && N == 0)) {
     err = "BVH: bad triangle or node count";
@@ -515,7 +596,7 @@ bool bvh_from_reference(int T, const float *v0, const float *v1, const float *v2
       out.ref_link[i] = make_int4(left[i], right[i], 0, 0);
     }
   }
-  return flatten_two_child(std::move(tree), prims, out.perm, out, err, width);
+  return flatten_two_child(std::move(tree), prims, out.perm, out, err, width, quantize);
 }
 
 }  // namespace ts

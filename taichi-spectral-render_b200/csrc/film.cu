@@ -145,7 +145,9 @@ cudaError_t launch_resolve_rgb(Film f, const float *cmf, double scale, const flo
 cudaError_t launch_render_normals(const DevScene &s, const DevConfig &c, float *out, uint32_t *err,
                                   cudaStream_t st) {
   const int g = grid_for((size_t)c.W * c.H);
-  if (s.node_width == 8) k_normals<8><<<g, kThreads, 0, st>>>(s, c, out, err);
+  if (s.node_width == 9) k_normals<9><<<g, kThreads, 0, st>>>(s, c, out, err);
+  else if (s.node_width == 5) k_normals<5><<<g, kThreads, 0, st>>>(s, c, out, err);
+  else if (s.node_width == 8) k_normals<8><<<g, kThreads, 0, st>>>(s, c, out, err);
   else if (s.node_width == 4) k_normals<4><<<g, kThreads, 0, st>>>(s, c, out, err);
   else k_normals<2><<<g, kThreads, 0, st>>>(s, c, out, err);
   return cudaGetLastError();
@@ -155,6 +157,8 @@ cudaError_t launch_trace_batch(const DevScene &s, float eps, const float *rays, 
   if (n <= 0) return cudaSuccess;
   const int g = grid_for((size_t)n);
   if (mode != 0) k_trace_batch<1, 2><<<g, kThreads, 0, st>>>(s, eps, rays, n, tri_orig, t, u, v, err);
+  else if (s.node_width == 9) k_trace_batch<0, 9><<<g, kThreads, 0, st>>>(s, eps, rays, n, tri_orig, t, u, v, err);
+  else if (s.node_width == 5) k_trace_batch<0, 5><<<g, kThreads, 0, st>>>(s, eps, rays, n, tri_orig, t, u, v, err);
   else if (s.node_width == 8) k_trace_batch<0, 8><<<g, kThreads, 0, st>>>(s, eps, rays, n, tri_orig, t, u, v, err);
   else if (s.node_width == 4) k_trace_batch<0, 4><<<g, kThreads, 0, st>>>(s, eps, rays, n, tri_orig, t, u, v, err);
   else k_trace_batch<0, 2><<<g, kThreads, 0, st>>>(s, eps, rays, n, tri_orig, t, u, v, err);

@@ -118,7 +118,9 @@ namespace {
 template <int kMin>
 void launch_render_batch(BatchSlot *slots, int n, BatchHeader *h, uint32_t *err, int width, int grid, int block,
                          size_t smem, cudaStream_t st) {
-  if (width == 8) k_render_batch<8, kMin><<<grid, block, smem, st>>>(slots, n, h, err);
+  if (width == 9) k_render_batch<9, kMin><<<grid, block, smem, st>>>(slots, n, h, err);
+  else if (width == 5) k_render_batch<5, kMin><<<grid, block, smem, st>>>(slots, n, h, err);
+  else if (width == 8) k_render_batch<8, kMin><<<grid, block, smem, st>>>(slots, n, h, err);
   else if (width == 4) k_render_batch<4, kMin><<<grid, block, smem, st>>>(slots, n, h, err);
   else if (width == 3) k_render_batch<3, kMin><<<grid, block, smem, st>>>(slots, n, h, err);
   else k_render_batch<2, kMin><<<grid, block, smem, st>>>(slots, n, h, err);
@@ -156,6 +158,10 @@ cudaError_t batch_set_smem_limit(int n) {
         cudaFuncSetAttribute(k_render_batch<3, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
         cudaFuncSetAttribute(k_render_batch<4, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
         cudaFuncSetAttribute(k_render_batch<8, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
+        cudaFuncSetAttribute(k_render_batch<5, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
+        cudaFuncSetAttribute(k_render_batch<9, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
+        cudaFuncSetAttribute(k_render_batch<5, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
+        cudaFuncSetAttribute(k_render_batch<9, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
         cudaFuncSetAttribute(k_render_batch<2, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
         cudaFuncSetAttribute(k_render_batch<3, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
         cudaFuncSetAttribute(k_render_batch<4, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),

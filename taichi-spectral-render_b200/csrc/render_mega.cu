@@ -87,7 +87,9 @@ cudaError_t launch_render_mega(const DevScene &s, const DevConfig &c, uint32_t p
   cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), st);
   if (e != cudaSuccess) return e;
   block = block > 128 ? 128 : block;  // the kernel is compiled for blocks of at most 128 threads
-  if (s.node_width == 8) launch_w<8>(s, c, pass, npass, band, f, counter, err, grid, block, st, work, occupancy);
+  if (s.node_width == 9) launch_w<9>(s, c, pass, npass, band, f, counter, err, grid, block, st, work, occupancy);
+  else if (s.node_width == 5) launch_w<5>(s, c, pass, npass, band, f, counter, err, grid, block, st, work, occupancy);
+  else if (s.node_width == 8) launch_w<8>(s, c, pass, npass, band, f, counter, err, grid, block, st, work, occupancy);
   else if (s.node_width == 4) launch_w<4>(s, c, pass, npass, band, f, counter, err, grid, block, st, work, occupancy);
   else if (c.speculative) launch_w<3>(s, c, pass, npass, band, f, counter, err, grid, block, st, work, occupancy);
   else launch_w<2>(s, c, pass, npass, band, f, counter, err, grid, block, st, work, occupancy);

@@ -183,7 +183,11 @@ template <bool kLoop = false>
 void launch_trace(const DevScene &s, const DevConfig &c, int depth, Film f, const WaveBuffers &w, uint32_t *err,
                   int grid, int block, cudaStream_t st, int budget, int ext_sorted = 0, int shadow_sorted = 0,
                   WaveLoop *L = nullptr) {
-  if (s.node_width == 8)
+  if (s.node_width == 9)
+    k_trace<9, kLoop><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget, ext_sorted, shadow_sorted, L);
+  else if (s.node_width == 5)
+    k_trace<5, kLoop><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget, ext_sorted, shadow_sorted, L);
+  else if (s.node_width == 8)
     k_trace<8, kLoop><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget, ext_sorted, shadow_sorted, L);
   else if (s.node_width == 4)
     k_trace<4, kLoop><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget, ext_sorted, shadow_sorted, L);
@@ -901,7 +905,9 @@ namespace {
 
 cudaError_t launch_trace_bloop(const BatchSlot *slots, const WaveBuffers &w, uint32_t *err, int width, int grid,
                                int block, int budget, cudaStream_t st) {
-  if (width == 8) k_trace_bloop<8><<<grid, block, 0, st>>>(slots, w, err, budget, w.loop);
+  if (width == 9) k_trace_bloop<9><<<grid, block, 0, st>>>(slots, w, err, budget, w.loop);
+  else if (width == 5) k_trace_bloop<5><<<grid, block, 0, st>>>(slots, w, err, budget, w.loop);
+  else if (width == 8) k_trace_bloop<8><<<grid, block, 0, st>>>(slots, w, err, budget, w.loop);
   else if (width == 4) k_trace_bloop<4><<<grid, block, 0, st>>>(slots, w, err, budget, w.loop);
   else if (width == 3) k_trace_bloop<3><<<grid, block, 0, st>>>(slots, w, err, budget, w.loop);
   else k_trace_bloop<2><<<grid, block, 0, st>>>(slots, w, err, budget, w.loop);

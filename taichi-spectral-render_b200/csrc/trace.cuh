@@ -362,14 +362,122 @@ TS_D bool trav_steps_wide(const DevScene &s, Traversal &t, int2 *stack, float ep
   return t.node == kTravDone;
 }
 
-// Dispatch on the node width (a compile-time choice of each kernel instance).
+// ---- quantized wide nodes (layout ids 5: 4 children in 64 B, 9: 8 children in 96 B)
+// float4 0 = (origin.xyz, biased scale exponents x, y, z and the child count as
+// bytes); then the child refs; then the child boxes as bytes q per plane
+// (lo.x hi.x lo.y hi.y lo.z hi.z, one byte per child) with bound = origin + q *
+// 2^e, decoded with one IEEE multiply (exact) and one add.  The host rounded
+// every byte outwards against exactly this decode, so a decoded box contains
+// the exact one: the slab test accepts at least the rays the exact box would,
+// entry distances are no larger, and culling stays conservative -- the
+// closest hit is the same as with full-precision boxes.
+template <int WQ, bool kCount = false>
+TS_D bool trav_steps_q(const DevScene &s, Traversal &t, int2 *stack, float eps, int budget, uint32_t &errbits,
+                       TraceCount *tc = nullptr) {
+  constexpr int N = WQ == 9 ? 8 : 4;  // children per node
+  constexpr int R = N / 4;            // float4s of refs (and 32-bit words per byte plane)
+  constexpr int F = WQ == 9 ? 6 : 4;  // float4s per node
+  for (int it = 0; it < budget; ++it) {
+    if (t.node == kTravDone) return true;
+    if (t.node >= 0) {
+      const float4 *n = s.node + (size_t)F * t.node;
+      if (kCount) tc->nodes++;
+      const float4 h = __ldg(n);
+      const uint32_t meta = __float_as_uint(h.w);
+      const float sx = __uint_as_float((meta & 0xffu) << 23);
+      const float sy = __uint_as_float(((meta >> 8) & 0xffu) << 23);
+      const float sz = __uint_as_float(((meta >> 16) & 0xffu) << 23);
+      const int nc = (int)(meta >> 24);
+      int ref[N];
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        const int4 l = __ldg(reinterpret_cast<const int4 *>(n + 1 + q));
+        ref[4 * q + 0] = l.x; ref[4 * q + 1] = l.y; ref[4 * q + 2] = l.z; ref[4 * q + 3] = l.w;
+      }
+      uint32_t wq[6 * R];  // plane r, children 4j..4j+3 in word r * R + j
+      {
+        const uint4 *b = reinterpret_cast<const uint4 *>(n + 1 + R);
+#pragma unroll
+        for (int i = 0; i < (6 * R + 3) / 4; ++i) {
+          const uint4 v = __ldg(b + i);
+          if (4 * i + 0 < 6 * R) wq[4 * i + 0] = v.x;
+          if (4 * i + 1 < 6 * R) wq[4 * i + 1] = v.y;
+          if (4 * i + 2 < 6 * R) wq[4 * i + 2] = v.z;
+          if (4 * i + 3 < 6 * R) wq[4 * i + 3] = v.w;
+        }
+      }
+      float key[N];
+      int nh = 0;
+#pragma unroll
+      for (int k = 0; k < N; ++k) {
+        const int j = k >> 2, sh = 8 * (k & 3);
+        const float lox = xadd(h.x, xmul((float)((wq[0 * R + j] >> sh) & 0xffu), sx));
+        const float hix = xadd(h.x, xmul((float)((wq[1 * R + j] >> sh) & 0xffu), sx));
+        const float loy = xadd(h.y, xmul((float)((wq[2 * R + j] >> sh) & 0xffu), sy));
+        const float hiy = xadd(h.y, xmul((float)((wq[3 * R + j] >> sh) & 0xffu), sy));
+        const float loz = xadd(h.z, xmul((float)((wq[4 * R + j] >> sh) & 0xffu), sz));
+        const float hiz = xadd(h.z, xmul((float)((wq[5 * R + j] >> sh) & 0xffu), sz));
+        float te, tx;
+        box_hit(lox, hix, loy, hiy, loz, hiz, t.o, t.inv, te, tx);
+        const bool hit = k < nc && te < tx && tx > 0.f && te <= t.tcull;
+        key[k] = hit ? te : INFINITY;
+        nh += hit;
+      }
+      if (nh > 0) {
+        sort_children<N>(key, ref);
+        if (t.sp + nh - 1 <= kWideStack) {
+#pragma unroll
+          for (int k = N - 1; k >= 1; --k)
+            if (k < nh) stack[t.sp++] = make_int2(ref[k], __float_as_int(key[k]));
+        } else {
+          errbits |= kErrStackOverflow;
+        }
+        t.node = ref[0];
+        continue;
+      }
+    } else {
+      const int code = ~t.node;
+      const int first = code >> 4;
+      const int cnt = (code & 15) + 1;
+      if (kCount) tc->tris += cnt;
+      for (int i = 0; i < cnt; ++i) {
+        const float4 *tp = s.tri + 3 * (size_t)(first + i);
+        const float4 A = __ldg(tp + 0), E1 = __ldg(tp + 1), E2 = __ldg(tp + 2);
+        float u, v;
+        const float tt = tri_hit(t.o, t.d, A, E1, E2, eps, u, v);
+        if (tt > eps && tt < t.h.t) {
+          t.h.t = tt;
+          t.h.u = u;
+          t.h.v = v;
+          t.h.slot = first + i;
+          t.tcull = fminf(t.tcull, cull_bound(tt));
+        }
+      }
+    }
+    for (;;) {
+      if (t.sp == 0) {
+        t.node = kTravDone;
+        return true;
+      }
+      const int2 e = stack[--t.sp];
+      if (__int_as_float(e.y) <= t.tcull) {
+        t.node = e.x;
+        break;
+      }
+    }
+  }
+  return t.node == kTravDone;
+}
+
+// Dispatch on the node layout (a compile-time choice of each kernel instance).
 // W = 2: two-child if-if loop; W = 3: two-child speculative while-while (same
-// layout); W = 4 / 8: wide nodes.
+// layout); W = 4 / 8: wide nodes; W = 5 / 9: quantized 4- / 8-wide nodes.
 template <int W, bool kCount = false>
 TS_D bool trav_advance(const DevScene &s, Traversal &t, int2 *stack, float eps, int budget, uint32_t &errbits,
                        TraceCount *tc = nullptr) {
   if (W == 2) return trav_steps<kCount>(s, t, stack, eps, budget, errbits, tc);
   if (W == 3) return trav_steps_spec<kCount>(s, t, stack, eps, budget, errbits, tc);
+  if (W == 5 || W == 9) return trav_steps_q<W, kCount>(s, t, stack, eps, budget, errbits, tc);
   return trav_steps_wide<W, kCount>(s, t, stack, eps, budget, errbits, tc);
 }
 

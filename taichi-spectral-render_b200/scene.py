@@ -177,6 +177,7 @@ class CompiledScene:
         d.bvh_cost_trav = float(p.get("cost_trav", 0.0))
         d.bvh_cost_tri = float(p.get("cost_tri", 0.0))
         d.bvh_width = int(p.get("width", 0))
+        d.bvh_quantized = 1 if p.get("quantize", False) else 0
         return d
 
 

@@ -59,13 +59,14 @@ def terrain():
     return dict(s=s, c=c, ex=ex, comp=comp, bvh=bvh, rays=rays, tri_o=tri_o, t_o=t_o)
 
 
-@pytest.mark.parametrize("node_width", [2, 4, 8])
-def test_full_size_terrain_closest_hits(terrain, node_width):
+@pytest.mark.parametrize("node_width,quantize", [(2, False), (4, False), (8, False), (4, True), (8, True)])
+def test_full_size_terrain_closest_hits(terrain, node_width, quantize):
     T = terrain
     rays = T["rays"]
     assert rays.shape[0] > 1_000_000
-    with renderer_for(T["comp"], T["bvh"], T["s"]["camera"], node_width=node_width) as r:
+    with renderer_for(T["comp"], T["bvh"], T["s"]["camera"], node_width=node_width, quantize=quantize) as r:
         assert r.scene_info()["node_width"] == node_width
+        assert r.scene_info()["node_quantized"] == int(quantize)
         tri, t, _, _ = (x.cpu().numpy() for x in r.trace(torch.from_numpy(rays).cuda(), "fast"))
         if node_width == 4:
             k = 131072  # the exact reference-order kernel on a share of the rays

@@ -9,11 +9,11 @@ from spectral_b200 import configs
 pytestmark = pytest.mark.gpu
 
 
-def renderer_for(compiled, bvh, cam, node_width=0, **kw):
+def renderer_for(compiled, bvh, cam, node_width=0, quantize=False, **kw):
     """A Renderer over an already compiled scene (no scene dictionary needed)."""
     import ctypes
     cfg = sb.RenderConfig(width=kw.get("width", 16), height=kw.get("height", 16), kernel=kw.get("kernel", "mega"))
-    compiled.bvh_params = dict(compiled.bvh_params, width=node_width)
+    compiled.bvh_params = dict(compiled.bvh_params, width=node_width, quantize=quantize)
     r = sb.Renderer.__new__(sb.Renderer)
     r.config, r.lib, r._ctx = cfg, sb.load(), ctypes.c_void_p()
     sb._lib.check(r.lib.ts_create(ctypes.byref(cfg.to_c()), ctypes.byref(r._ctx)))
@@ -55,14 +55,15 @@ def _near_tie_check(tri, t, tri_o, t_o):
     return int(mism.sum())
 
 
-@pytest.mark.parametrize("node_width", [2, 4, 8])
-def test_fast_traversal_matches_except_near_ties(node_width):
+@pytest.mark.parametrize("node_width,quantize", [(2, False), (4, False), (8, False), (4, True), (8, True)])
+def test_fast_traversal_matches_except_near_ties(node_width, quantize):
     cs, bvh, cam = golden_compiled()
     sc = oracle_scene(cs, bvh, cam)
     rays = np.concatenate([random_rays(100000, 2), camera_rays(cam, 200, 200, jitter_seed=1)], 0)
     tri_o, t_o, _, _ = oracle_hits(sc, rays, bvh["tri_perm"])
-    with renderer_for(cs, bvh, cam, node_width=node_width) as r:
+    with renderer_for(cs, bvh, cam, node_width=node_width, quantize=quantize) as r:
         assert r.scene_info()["node_width"] == node_width
+        assert r.scene_info()["node_quantized"] == int(quantize)
         tri, t, _, _ = (x.cpu().numpy() for x in r.trace(torch.from_numpy(rays).cuda(), "fast"))
     ties = _near_tie_check(tri, t, tri_o, t_o)
     assert ties <= 0.002 * len(rays)
@@ -89,8 +90,8 @@ def test_binned_bvh_traversal_matches_reference_semantics(node_width):
                 assert _near_tie_check(tri, t, tri_o, t_o) <= 0.002 * len(rays)
 
 
-@pytest.mark.parametrize("node_width", [2, 4, 8])
-def test_misses_and_degenerate_rays(node_width):
+@pytest.mark.parametrize("node_width,quantize", [(2, False), (4, False), (8, False), (4, True), (8, True)])
+def test_misses_and_degenerate_rays(node_width, quantize):
     cs, bvh, cam = golden_compiled()
     sc = oracle_scene(cs, bvh, cam)
     # outward rays from outside the box, axis-parallel rays, rays starting on a wall
@@ -98,22 +99,23 @@ def test_misses_and_degenerate_rays(node_width):
                      [0, -1, 0, 0, 1, 0], [0.3, 0.99, 0.3, 0, -1, 0], [2, 2, 2, 1, 1, 1]], np.float32)
     rays[:, 3:] /= np.linalg.norm(rays[:, 3:], axis=1, keepdims=True)
     tri_o, t_o, _, _ = oracle_hits(sc, rays, bvh["tri_perm"])
-    with renderer_for(cs, bvh, cam, node_width=node_width) as r:
+    with renderer_for(cs, bvh, cam, node_width=node_width, quantize=quantize) as r:
         for mode in ("fast", "reference_order"):
             tri, t, _, _ = (x.cpu().numpy() for x in r.trace(torch.from_numpy(rays).cuda(), mode))
             assert np.array_equal(tri, tri_o) and np.array_equal(t, t_o), mode
     assert tri_o[0] == -1 and t_o[0] == np.float32(1e9)
 
 
-@pytest.mark.parametrize("node_width", [2, 4, 8])
-def test_large_mesh_traversal_matches_oracle(node_width):
+@pytest.mark.parametrize("node_width,quantize", [(2, False), (4, False), (8, False), (4, True), (8, True)])
+def test_large_mesh_traversal_matches_oracle(node_width, quantize):
     s, c, ex = configs.terrain_scene(grid=256, sphere_slices=100, sphere_stacks=101)
     comp = sb.compile_scene(s, c.bands, eems=ex["eems"], cmf=ex["cmf"])
     bvh = sb._lib.build_bvh_host(comp.tris["v0"], comp.tris["v1"], comp.tris["v2"])
     sc = oracle_scene(comp, bvh, s["camera"])
     rays = camera_rays(s["camera"], 256, 256, fov_scale=c.fov_scale, jitter_seed=3)
     tri_o, t_o, _, _ = oracle_hits(sc, rays, bvh["tri_perm"])
-    with renderer_for(comp, bvh, s["camera"], node_width=node_width) as r:
+    with renderer_for(comp, bvh, s["camera"], node_width=node_width, quantize=quantize) as r:
+        assert r.scene_info()["node_quantized"] == int(quantize)
         tri, t, _, _ = (x.cpu().numpy() for x in r.trace(torch.from_numpy(rays).cuda(), "fast"))
         assert r.check_device() == 0
     assert _near_tie_check(tri, t, tri_o, t_o) <= 0.002 * len(rays)
