@@ -45,7 +45,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--kernel", default="mega", choices=["mega", "wavefront"])
-    p.add_argument("--workload", default="terrain", choices=["terrain", "box", "volume", "batch", "adjoint", "rmse"])
+    p.add_argument("--workload", default="terrain", choices=["terrain", "box", "volume", "batch", "adjoint", "rmse", "gradcheck"])
     p.add_argument("--width", type=int, default=2, choices=[2, 4, 8], help="BVH node width")
     p.add_argument("--quantize", action="store_true", help="4- / 8-wide nodes with 8-bit child boxes (--no-tune)")
     p.add_argument("--traversal", default="default", choices=["default", "speculative"])
@@ -67,6 +67,8 @@ def parse():
     p.add_argument("--batch-scenes", type=int, default=64, help="scenes of the batched workload (--workload batch)")
     p.add_argument("--batch-target", type=float, default=0.05, help="RMSE target of the batched workload")
     p.add_argument("--passes", type=int, default=25, help="passes per adjoint launch (--workload adjoint)")
+    p.add_argument("--gradcheck-blocks", type=int, default=40, help="blocks per evaluation (--workload gradcheck)")
+    p.add_argument("--gradcheck-res", type=int, default=128, help="resolution (--workload gradcheck)")
     return p.parse_args()
 
 
@@ -344,6 +346,37 @@ def plain_seconds(name, blocks, timed_blocks=6):
     return {"kernel": "depth-synchronous wavefront pass, one launch per pass (four-child nodes)",
             "seconds_per_block": per_block, "timed_blocks": n, "seconds_same_paths": per_block * blocks,
             "device_error_bits": bits}
+
+
+def bench_gradcheck(args):
+    """The adjoint of the inverse-rendering workload's 79 parameters against
+    central finite differences (h = 1e-3, common random numbers): the volume
+    scene (HG medium, fluorescent wall, depth 32), parameters of seed 8 (the
+    fit's starting point).  Prints one JSON line with every parameter."""
+    import numpy as np
+    import torch
+    import spectral_b200 as sb
+    from spectral_b200 import configs, inverse
+    res = args.gradcheck_res
+    s, c, ex = configs.volume_scene(width=res, height=res, depth=32)
+    c.kernel = "wavefront"
+    c.queue_capacity = c.bands * res * res
+    t0 = time.perf_counter()
+    with sb.Renderer(s, c, eems=ex["eems"], cmf=ex["cmf"]) as r:
+        p = inverse.Params.from_scene_params(inverse.scene_params(8), "cuda")
+        rows = inverse.gradient_check(r, p, h=1e-3, blocks=args.gradcheck_blocks)
+        bits = r.check_device()
+    secs = time.perf_counter() - t0
+    rel = np.array([abs(x["adjoint"] - x["fd"]) / max(abs(x["fd"]), 1e-300) for x in rows])
+    z = np.array([(x["adjoint"] - x["fd"]) / max(x["fd_sem"], 1e-300) for x in rows])
+    noise = np.array([x["fd_sem"] / max(abs(x["fd"]), 1e-300) for x in rows])
+    print(json.dumps({"metric": "adjoint vs central finite differences", "parameters": len(rows),
+                      "within_2pct": int((rel <= 0.02).sum()), "max_rel_err": float(rel.max()),
+                      "median_rel_err": float(np.median(rel)), "max_abs_z": float(np.abs(z).max()),
+                      "max_fd_rel_sem": float(noise.max()), "h": 1e-3, "blocks": args.gradcheck_blocks,
+                      "config": {"workload": f"volume scene (HG medium g 0.7, fluorescent wall) {res}x{res}, depth 32, "
+                                             "25 bands; 79 parameters of seed 8"},
+                      "seconds": secs, "device_error_bits": bits, "rows": rows}))
 
 
 def bench_rmse(args):
@@ -846,5 +879,7 @@ if __name__ == "__main__":
         bench_adjoint(a)
     elif a.workload == "rmse":
         bench_rmse(a)
+    elif a.workload == "gradcheck":
+        bench_gradcheck(a)
     else:
         bench_ours(a)
