@@ -28,11 +28,11 @@ def oracle_passes(comp, bvh, scene, cfg, passes, use_double=False):
 
 
 def gpu_passes(scene, cfg, ex, bvh, kernel, passes, sort_keys=0, node_width=0, traversal="default",
-               queue_capacity=0):
+               queue_capacity=0, quantize=False):
     c2 = sb.RenderConfig(**{**cfg.__dict__, "kernel": kernel, "sort_keys": sort_keys, "traversal": traversal,
                             "queue_capacity": queue_capacity})
     with sb.Renderer(scene, c2, eems=ex["eems"], cmf=ex["cmf"], bvh=bvh,
-                     bvh_params={"width": node_width}) as r:
+                     bvh_params={"width": node_width, "quantize": quantize}) as r:
         for p in passes:
             r.cast_rays(p % cfg.bands, pass_idx=p)
         g = r.block_film.cpu().numpy().reshape(cfg.bands, -1).T.copy()
@@ -67,6 +67,21 @@ def test_volume_fluorescence_common_random_numbers(kernel, node_width):
     passes = range(25)
     crn_agreement(gpu_passes(s, c, ex, bvh, kernel, passes, node_width=node_width),
                   oracle_passes(comp, bvh, s, c, passes))
+
+
+@pytest.mark.parametrize("kernel,node_width,quantize,qcap", [("mega", 2, False, 0), ("wavefront", 4, False, 0),
+                                                             ("wavefront", 4, True, 64 * 64 * 25),
+                                                             ("mega", 8, True, 0)])
+def test_opaque_terrain_common_random_numbers(kernel, node_width, quantize, qcap):
+    """An opaque scene (GGX conductors only): shadow segments stop at the first
+    occluder closer than the light (no material could let light through it),
+    with the same deposits as the reference's closest-hit shadow chain."""
+    s, c, ex, comp, bvh = setup(configs.terrain_scene, grid=96, sphere_slices=40, sphere_stacks=41, width=64,
+                                height=64)
+    passes = range(25)
+    g = gpu_passes(s, c, ex, bvh, kernel, passes, node_width=node_width, quantize=quantize, queue_capacity=qcap)
+    crn_agreement(g, oracle_passes(comp, bvh, s, c, passes))
+    assert g.sum() > 0
 
 
 def test_reference_scene_common_random_numbers():
