@@ -185,11 +185,15 @@ class Renderer:
         if not p:
             return
         self._pending = []
-        first_pass, first_band = p[0]
-        if len(p) == 1:
-            self._check(self.lib.ts_render_pass(self._ctx, first_pass, first_band, _stream()))
-        else:
-            self._check(self.lib.ts_render_passes(self._ctx, first_pass, len(p), first_band, _stream()))
+        # one launch holds at most 2^31 - 1 paths: very large frames launch the run in chunks
+        per = max(1, (2 ** 31 - 1) // max(1, self.config.width * self.config.height))
+        for k in range(0, len(p), per):
+            first_pass, first_band = p[k]
+            n = min(per, len(p) - k)
+            if n == 1:
+                self._check(self.lib.ts_render_pass(self._ctx, first_pass, first_band, _stream()))
+            else:
+                self._check(self.lib.ts_render_passes(self._ctx, first_pass, n, first_band, _stream()))
 
     def set_launch_config(self, kernel=None, traversal=None, block_size=None, blocks_per_sm=None, sort_keys=None,
                           trace_budget=None, occupancy=None, queue_capacity=None, loop_host=None):

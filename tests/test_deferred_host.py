@@ -110,3 +110,16 @@ def test_without_deferral_every_pass_launches(make):
     for k in range(3):
         r.cast_rays(k)
     assert r.lib.launches() == [("pass", 0, 0), ("pass", 1, 1), ("pass", 2, 2)]
+
+
+def test_huge_frames_flush_in_chunks_under_the_launch_limit(make):
+    """A block whose paths exceed what one launch may hold (2^31 - 1) is
+    launched in chunks of whole passes -- the same passes, no failure."""
+    r = make(bands=25)
+    r.config = rmod.RenderConfig(width=9500, height=9500, bands=25, defer_passes=True)
+    for k in range(25):
+        r.cast_rays(k)
+    got = [c for c in r.lib.launches() if c[0] in ("pass", "bundle")]
+    per = (2 ** 31 - 1) // (9500 * 9500)
+    assert per == 23
+    assert got == [("bundle", 0, 23, 0), ("bundle", 23, 2, 23)]
