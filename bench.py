@@ -45,7 +45,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--kernel", default="mega", choices=["mega", "wavefront"])
-    p.add_argument("--workload", default="terrain", choices=["terrain", "box", "volume", "batch", "adjoint", "rmse", "gradcheck"])
+    p.add_argument("--workload", default="terrain", choices=["terrain", "box", "volume", "batch", "adjoint", "rmse", "gradcheck", "inverse"])
     p.add_argument("--width", type=int, default=2, choices=[2, 4, 8], help="BVH node width")
     p.add_argument("--quantize", action="store_true", help="4- / 8-wide nodes with 8-bit child boxes (--no-tune)")
     p.add_argument("--traversal", default="default", choices=["default", "speculative"])
@@ -69,6 +69,7 @@ def parse():
     p.add_argument("--passes", type=int, default=25, help="passes per adjoint launch (--workload adjoint)")
     p.add_argument("--gradcheck-blocks", type=int, default=40, help="blocks per evaluation (--workload gradcheck)")
     p.add_argument("--gradcheck-res", type=int, default=128, help="resolution (--workload gradcheck)")
+    p.add_argument("--iterations", type=int, default=200, help="Adam iterations (--workload inverse)")
     return p.parse_args()
 
 
@@ -377,6 +378,55 @@ def bench_gradcheck(args):
                       "config": {"workload": f"volume scene (HG medium g 0.7, fluorescent wall) {res}x{res}, depth 32, "
                                              "25 bands; 79 parameters of seed 8"},
                       "seconds": secs, "device_error_bits": bits, "rows": rows}))
+
+
+def bench_inverse(args):
+    """The differentiable inverse-rendering workload as configured: the volume
+    scene at 256x256 (depth 32), 79 parameters, target image at 4,100 spp from
+    the hidden parameters of seed 7, start from seed 8, 2 blocks (50 passes) per
+    forward and adjoint, Adam lr 1e-2 for --iterations steps.  Reports the loss
+    history, seconds per iteration, the final image's relative XYZ RMSE
+    against the target image, the noise floor (the hidden parameters' own
+    loss) and the parameter errors."""
+    import torch
+    import spectral_b200 as sb
+    from spectral_b200 import configs, inverse
+    s, c, ex = configs.volume_scene(width=256, height=256, depth=32)
+    c.kernel = "wavefront"
+    c.queue_capacity = c.bands * 256 * 256
+    with sb.Renderer(s, c, eems=ex["eems"], cmf=ex["cmf"]) as r:
+        hidden = inverse.Params.from_scene_params(inverse.scene_params(7), "cuda")
+        init = inverse.Params.from_scene_params(inverse.scene_params(8), "cuda")
+        t0 = time.perf_counter()
+        target = inverse.render_target(r, hidden, blocks=164)  # 4,100 spp
+        torch.cuda.synchronize()
+        t_target = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        fit, hist = inverse.run(r, target, init, iterations=args.iterations, lr=1e-2, blocks=2)
+        torch.cuda.synchronize()
+        t_fit = time.perf_counter() - t0
+
+        def image_rmse(p, blocks=40):
+            """relative XYZ RMSE of p's image (blocks spectral blocks) against the target"""
+            x = inverse.render_target(r, p, blocks=blocks)
+            return float(torch.linalg.vector_norm(x - target) / torch.linalg.vector_norm(target))
+
+        e_init, e_fit, e_hidden = image_rmse(init), image_rmse(fit), image_rmse(hidden)
+        floor = inverse.image_loss(r, hidden, target)
+        bits = r.check_device()
+    print(json.dumps({"metric": "inverse rendering: relative XYZ RMSE of the fitted image against the target",
+                      "value": e_fit, "unit": "relative RMSE", "higher_is_better": False,
+                      "config": {"workload": "volume scene 256x256, depth 32, 25 bands; 79 parameters (2x25 wall "
+                                             "albedos, 25-band sigma_a, g, 3 roughnesses); target 4,100 spp of "
+                                             "seed 7, start seed 8, Adam lr 1e-2, 50 passes per forward and adjoint",
+                                 "iterations": args.iterations},
+                      "image_rmse": {"init": e_init, "fitted": e_fit, "hidden_params_at_same_spp": e_hidden},
+                      "loss": {"first": hist[0], "last": hist[-1], "noise_floor": floor,
+                               "history_every_10": hist[::10]},
+                      "seconds_per_iteration": t_fit / args.iterations, "target_seconds": t_target,
+                      "parameter_error": {"init": inverse.parameter_error(init, hidden),
+                                          "fitted": inverse.parameter_error(fit, hidden)},
+                      "device_error_bits": bits}))
 
 
 def bench_rmse(args):
@@ -881,5 +931,7 @@ if __name__ == "__main__":
         bench_rmse(a)
     elif a.workload == "gradcheck":
         bench_gradcheck(a)
+    elif a.workload == "inverse":
+        bench_inverse(a)
     else:
         bench_ours(a)
