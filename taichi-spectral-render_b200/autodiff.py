@@ -30,7 +30,8 @@ class _RenderFilm(torch.autograd.Function):
         r.update_materials(mat, em)
         r.clear_pixel_space()
         B = r.config.bands
-        r.record_paths(first_pass, num_blocks * B)  # the adjoint then skips its weight replay
+        # records let the adjoint skip its weight replay; only worth it when a gradient will follow
+        r.record_paths(first_pass, num_blocks * B if any(ctx.needs_input_grad[:2]) else 0)
         for blk in range(num_blocks):
             r.cast_rays_bundle(0, B, pass_idx=first_pass + blk * B)  # one launch per block
             r.average_and_reset_block(blk + 1)
