@@ -427,9 +427,6 @@ ts_status ts_upload_scene(ts_ctx *c, const ts_scene_desc *sd) {
   ds.num_lights = d_nl;
   ds.light_area = d_larea;
   ds.max_lights = L;
-  ds.opaque = 1;
-  for (size_t i = 0; i < (size_t)M * B; ++i)
-    if (sd->mat_i32[(i / B) * 2 * B + (i % B)]) ds.opaque = 0;  // is_true_volume of (material, band)
   c->ds = ds;
   c->d_cmf = d_cmf;
   c->perm = bvh.perm;

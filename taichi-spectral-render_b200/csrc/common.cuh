@@ -71,7 +71,6 @@ struct DevScene {
   const float *__restrict__ light_area;    // [B]
   int32_t max_lights;
   float3 cam_o, cam_u, cam_v, cam_w;
-  int32_t opaque;  // no material is a true volume at any band: shadow segments end at their first occluder
 };
 
 // ------------------------------------------------------------ float3 helpers

@@ -97,8 +97,7 @@ __device__ __forceinline__ bool mega_vertex(const DevScene &s, const DevConfig &
       ss.seg = 0;
       for (;;) {
         const Hit sh =
-            trace_closest<W, kCount>(s, ss.pos, q.dir, c.eps, errbits, &cnt.tc, shadow_bound(s, c, q, ss, p.active),
-                                     q.light_slot, q.max_dist - ss.traveled);
+            trace_closest<W, kCount>(s, ss.pos, q.dir, c.eps, errbits, &cnt.tc, shadow_bound(s, c, q, ss, p.active));
         if (kCount) {
           cnt.trace++;
           cnt.hit += sh.slot >= 0 && sh.slot != q.light_slot;

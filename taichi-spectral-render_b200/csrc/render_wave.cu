@@ -152,8 +152,7 @@ __global__ void __launch_bounds__(kMaxBlock, 4) k_trace(DevScene s, DevConfig c,
           ss.traveled = 0.f;
           ss.vol = sq.vol;
           ss.seg = 0;
-          trav_begin_shadow(s, t, ss.pos, sq.dir, shadow_bound(s, c, sq, ss, band), sq.light_slot,
-                            sq.max_dist - ss.traveled, c.eps);
+          trav_begin(s, t, ss.pos, sq.dir, shadow_bound(s, c, sq, ss, band));
         } else {
           item = idx;
           pid = q[idx - nsh];
@@ -169,8 +168,7 @@ __global__ void __launch_bounds__(kMaxBlock, 4) k_trace(DevScene s, DevConfig c,
           if (ss.total > 1e-6f) deposit(f, pixel, dep_band, sq.contrib * ss.total, shared);
           item = -1;
         } else {
-          trav_begin_shadow(s, t, ss.pos, sq.dir, shadow_bound(s, c, sq, ss, band), sq.light_slot,
-                            sq.max_dist - ss.traveled, c.eps);
+          trav_begin(s, t, ss.pos, sq.dir, shadow_bound(s, c, sq, ss, band));
         }
       } else {
         w.hit[pid] = make_float4(t.h.t, t.h.u, t.h.v, __int_as_float(t.h.slot));
@@ -815,8 +813,7 @@ __global__ void __launch_bounds__(kMaxBlock, 4) k_trace_bloop(const BatchSlot *_
           ss.traveled = 0.f;
           ss.vol = sq.vol;
           ss.seg = 0;
-          trav_begin_shadow(sl.s, t, ss.pos, sq.dir, shadow_bound(sl.s, sl.c, sq, ss, band), sq.light_slot,
-                            sq.max_dist - ss.traveled, sl.c.eps);
+          trav_begin(sl.s, t, ss.pos, sq.dir, shadow_bound(sl.s, sl.c, sq, ss, band));
         } else {
           item = idx;
           pid = q[idx - nsh];
@@ -834,8 +831,7 @@ __global__ void __launch_bounds__(kMaxBlock, 4) k_trace_bloop(const BatchSlot *_
           if (ss.total > 1e-6f) deposit(sl.f, pixel, dep_band, sq.contrib * ss.total, slot_shared(sl));
           item = -1;
         } else {
-          trav_begin_shadow(sl.s, t, ss.pos, sq.dir, shadow_bound(sl.s, sl.c, sq, ss, band), sq.light_slot,
-                            sq.max_dist - ss.traveled, sl.c.eps);
+          trav_begin(sl.s, t, ss.pos, sq.dir, shadow_bound(sl.s, sl.c, sq, ss, band));
         }
       } else {
         w.hit[pid] = make_float4(t.h.t, t.h.u, t.h.v, __int_as_float(t.h.slot));

@@ -78,18 +78,7 @@ struct Traversal {
   float tcull;
   Hit h;
   int node, sp;
-  // shadow segments of an opaque scene (trav_begin_shadow): a hit on another
-  // triangle than `alight` closer than `alimit` decides the segment, so the
-  // traversal stops there; alight == kNoAnyHit: closest hit only
-  int alight;
-  float alimit;
 };
-constexpr int kNoAnyHit = -2;
-
-// the first hit that ends an any-hit traversal (see Traversal)
-TS_D bool anyhit_stop(const Traversal &t, float tt, int slot) {
-  return t.alight != kNoAnyHit && tt < t.alimit && slot != t.alight;
-}
 
 // bound: distance beyond which hits do not matter to the caller.  Boxes past
 // it are skipped; a hit beyond it may still be returned (callers treat such a
@@ -104,28 +93,6 @@ TS_D void trav_begin(const DevScene &s, Traversal &t, float3 o, float3 d, float 
   t.tcull = cull_bound(fminf(bound, 1e9f));
   t.node = s.num_nodes > 0 ? 0 : kTravDone;
   t.sp = 0;
-  t.alight = kNoAnyHit;
-  t.alimit = 0.f;
-}
-
-// One shadow segment toward light triangle `light` with `remaining` distance
-// left (shadow_transmittance, main.py:1446-1499).  Its outcome depends only on
-// the closest hit h*: the light is reached if h*.t >= remaining or h* is the
-// light triangle; otherwise the surface decides, and in an opaque scene (no
-// true-volume material) every surface blocks, giving transmittance 0.  A hit
-// on another triangle closer than both `remaining` and the light triangle's
-// own hit distance t_L (tested here with the same function on the same ray,
-// so bit-identical to the traversal's test of it) proves h*.t < t_L and
-// h*.t < remaining, i.e. a blocked segment: the traversal may stop there.
-TS_D void trav_begin_shadow(const DevScene &s, Traversal &t, float3 o, float3 d, float bound, int light,
-                            float remaining, float eps) {
-  trav_begin(s, t, o, d, bound);
-  if (!s.opaque || light < 0) return;
-  const float4 *tp = s.tri + 3 * (size_t)light;
-  float u, v;
-  const float tl = tri_hit(o, d, __ldg(tp + 0), __ldg(tp + 1), __ldg(tp + 2), eps, u, v);
-  t.alight = light;
-  t.alimit = fminf(tl > eps ? tl : INFINITY, remaining);
 }
 
 // Advance by at most `budget` steps (one inner node, or one leaf and the pop
@@ -175,11 +142,6 @@ TS_D bool trav_steps(const DevScene &s, Traversal &t, int2 *stack, float eps, in
           t.h.v = v;
           t.h.slot = first + i;
           t.tcull = fminf(t.tcull, cull_bound(tt));
-          if (anyhit_stop(t, tt, first + i)) {
-            t.node = kTravDone;
-            t.sp = 0;
-            return true;
-          }
         }
       }
     }
@@ -281,11 +243,6 @@ TS_D bool trav_steps_spec(const DevScene &s, Traversal &t, int2 *stack, float ep
           t.h.v = v;
           t.h.slot = first + i;
           t.tcull = fminf(t.tcull, cull_bound(tt));
-          if (anyhit_stop(t, tt, first + i)) {
-            t.node = kTravDone;
-            t.sp = 0;
-            return true;
-          }
         }
       }
     }
@@ -387,11 +344,6 @@ TS_D bool trav_steps_wide(const DevScene &s, Traversal &t, int2 *stack, float ep
           t.h.v = v;
           t.h.slot = first + i;
           t.tcull = fminf(t.tcull, cull_bound(tt));
-          if (anyhit_stop(t, tt, first + i)) {
-            t.node = kTravDone;
-            t.sp = 0;
-            return true;
-          }
         }
       }
     }
@@ -499,11 +451,6 @@ TS_D bool trav_steps_q(const DevScene &s, Traversal &t, int2 *stack, float eps, 
           t.h.v = v;
           t.h.slot = first + i;
           t.tcull = fminf(t.tcull, cull_bound(tt));
-          if (anyhit_stop(t, tt, first + i)) {
-            t.node = kTravDone;
-            t.sp = 0;
-            return true;
-          }
         }
       }
     }
@@ -547,12 +494,10 @@ struct StackSize {
 // stalls dominated them when inlined).
 template <int W, bool kCount = false>
 __device__ __noinline__ Hit trace_closest(const DevScene &s, float3 o, float3 d, float eps, uint32_t &errbits,
-                                          TraceCount *tc = nullptr, float bound = 1e9f, int light = -1,
-                                          float remaining = 0.f) {
+                                          TraceCount *tc = nullptr, float bound = 1e9f) {
   Traversal t;
   int2 stack[StackSize<W>::value];
-  if (light >= 0) trav_begin_shadow(s, t, o, d, bound, light, remaining, eps);
-  else trav_begin(s, t, o, d, bound);
+  trav_begin(s, t, o, d, bound);
   trav_advance<W, kCount>(s, t, stack, eps, 0x7fffffff, errbits, tc);
   return t.h;
 }

@@ -153,10 +153,12 @@ def gradient_check(renderer, params, h=1e-3, blocks=40, first_pass=1 << 22, seed
     film).  Adjoint side: autodiff.render_film over ``blocks`` spectral blocks
     and backward through the parameter mapping of ``material_table``.
     Finite-difference side: L(theta + h e_i) and L(theta - h e_i) rendered on
-    the same passes (common random numbers), h absolute on each of the 79
-    physical parameters (albedos, sigma_a [1/m], g, roughnesses); the
-    per-block differences give the standard error of the estimate.  Returns a
-    list of dicts (name, index, adjoint, fd, fd_sem)."""
+    the same passes (common random numbers), with the step h relative to each
+    of the 79 physical parameters (albedos, sigma_a [1/m], g, roughnesses:
+    step h * |value|, so that no step leaves a parameter's domain -- sigma_a
+    spans orders of magnitude over the bands); the per-block differences give
+    the standard error of the estimate.  Returns a list of dicts (name, index,
+    value, step, adjoint, fd, fd_sem)."""
     r = renderer
     B = r.config.bands
     base = autodiff.material_table(r)
@@ -189,13 +191,14 @@ def gradient_check(renderer, params, h=1e-3, blocks=40, first_pass=1 << 22, seed
         for i in range(flat.numel()):
             lo = {n: getattr(params, n).detach().to(torch.float64) for n in NAMES}
             hi = dict(lo)
+            step = h * max(abs(float(flat[i])), 1e-12)
             dp = torch.zeros_like(flat)
-            dp[i] = h
+            dp[i] = step
             hi[name] = (flat + dp).reshape(val.shape)
             lo[name] = (flat - dp).reshape(val.shape)
-            d = (per_block(Params(**hi)) - per_block(Params(**lo))) / (2.0 * h)
-            rows.append({"name": name, "index": i, "adjoint": float(grad[i]), "fd": float(d.mean()),
-                         "fd_sem": float(d.std(ddof=1) / np.sqrt(blocks))})
+            d = (per_block(Params(**hi)) - per_block(Params(**lo))) / (2.0 * step)
+            rows.append({"name": name, "index": i, "value": float(flat[i]), "step": step, "adjoint": float(grad[i]),
+                         "fd": float(d.mean()), "fd_sem": float(d.std(ddof=1) / np.sqrt(blocks))})
     # leave the renderer with the unperturbed tables
     r.update_materials(material_table(base, params, lam).float().contiguous(), None)
     return rows

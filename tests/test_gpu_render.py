@@ -73,9 +73,9 @@ def test_volume_fluorescence_common_random_numbers(kernel, node_width):
                                                              ("wavefront", 4, True, 64 * 64 * 25),
                                                              ("mega", 8, True, 0)])
 def test_opaque_terrain_common_random_numbers(kernel, node_width, quantize, qcap):
-    """An opaque scene (GGX conductors only): shadow segments stop at the first
-    occluder closer than the light (no material could let light through it),
-    with the same deposits as the reference's closest-hit shadow chain."""
+    """An opaque scene (GGX conductors, a displaced sphere, eight area lights):
+    every node layout, both renderers and the regenerating loop against the
+    oracle with the same random streams."""
     s, c, ex, comp, bvh = setup(configs.terrain_scene, grid=96, sphere_slices=40, sphere_stacks=41, width=64,
                                 height=64)
     passes = range(25)

@@ -103,10 +103,17 @@ def test_misses_and_degenerate_rays(node_width, quantize):
         for mode in ("fast", "reference_order"):
             tri, t, _, _ = (x.cpu().numpy() for x in r.trace(torch.from_numpy(rays).cuda(), mode))
             if quantize and mode == "fast":
-                # the ray at (0.3, 0.99, 0.3) runs down the diagonal two floor triangles
-                # share: an exact tie, which the visit order of the quantized boxes breaks
-                # the other way (the parity rule counts ties instead of ordering them)
-                assert _near_tie_check(tri, t, tri_o, t_o) <= 1
+                # The ray from (0.3, 0.99, 0.3) straight down starts exactly on the x = 0.3
+                # plane of a sphere-triangle box: the reference's slab test computes
+                # 0 * inf = NaN there and rejects the box, missing the sphere hit at
+                # t = 1.409 (brute force finds it).  Quantized boxes are rounded outwards,
+                # so that plane no longer passes through the origin and the traversal finds
+                # the true closest hit.  Every other ray matches the reference exactly.
+                tri_b, t_b = orc.trace_brute(sc, oracle_config(sb.RenderConfig()), rays)
+                tri_b = np.where(tri_b >= 0, bvh["tri_perm"][np.maximum(tri_b, 0)], -1)
+                same = (tri == tri_o) & (t == t_o)
+                assert (same | (t == t_b)).all(), (tri, tri_o, tri_b)
+                assert same.sum() >= len(rays) - 1
             else:
                 assert np.array_equal(tri, tri_o) and np.array_equal(t, t_o), mode
     assert tri_o[0] == -1 and t_o[0] == np.float32(1e9)
