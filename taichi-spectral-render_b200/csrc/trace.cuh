@@ -362,6 +362,110 @@ TS_D bool trav_steps_wide(const DevScene &s, Traversal &t, int2 *stack, float ep
   return t.node == kTravDone;
 }
 
+// Speculative while-while traversal of the wide layout (Aila & Laine, HPG
+// 2009, as trav_steps_spec does for two-child nodes): a lane that reaches a
+// leaf postpones it and keeps descending; the warp tests leaves only once
+// every active lane holds one (or has finished).  Same results as
+// trav_steps_wide.
+template <int W, bool kCount = false>
+TS_D bool trav_steps_wide_spec(const DevScene &s, Traversal &t, int2 *stack, float eps, int budget,
+                               uint32_t &errbits, TraceCount *tc = nullptr) {
+  constexpr int P = W / 4;  // float4s per row
+  int leaf = 0;             // postponed leaf code (< 0), or 0
+  auto pop = [&]() {
+    t.node = kTravDone;
+    while (t.sp > 0) {
+      const int2 e = stack[--t.sp];
+      if (__int_as_float(e.y) <= t.tcull) {
+        t.node = e.x;
+        break;
+      }
+    }
+  };
+  for (int it = 0; it < budget; ++it) {
+    if (t.node == kTravDone && leaf == 0) return true;
+    // ---- inner nodes
+    while (t.node >= 0) {
+      const float4 *n = s.node + (size_t)(6 * P + P + (W == 4 ? 1 : 2)) * t.node;
+      if (kCount) tc->nodes++;
+      float row[6][W];
+#pragma unroll
+      for (int r = 0; r < 6; ++r)
+#pragma unroll
+        for (int q = 0; q < P; ++q) {
+          const float4 v = __ldg(n + r * P + q);
+          row[r][4 * q + 0] = v.x; row[r][4 * q + 1] = v.y; row[r][4 * q + 2] = v.z; row[r][4 * q + 3] = v.w;
+        }
+      int ref[W];
+#pragma unroll
+      for (int q = 0; q < P; ++q) {
+        const int4 l = __ldg(reinterpret_cast<const int4 *>(n + 6 * P + q));
+        ref[4 * q + 0] = l.x; ref[4 * q + 1] = l.y; ref[4 * q + 2] = l.z; ref[4 * q + 3] = l.w;
+      }
+      float key[W];
+      int nh = 0;
+#pragma unroll
+      for (int k = 0; k < W; ++k) {
+        float te, tx;
+        box_hit(row[0][k], row[1][k], row[2][k], row[3][k], row[4][k], row[5][k], t.o, t.inv, te, tx);
+        const bool h = te < tx && tx > 0.f && te <= t.tcull;
+        key[k] = h ? te : INFINITY;
+        nh += h;
+      }
+      if (nh > 0) {
+        sort_children<W>(key, ref);
+        if (t.sp + nh - 1 <= kWideStack) {
+#pragma unroll
+          for (int k = W - 1; k >= 1; --k)
+            if (k < nh) stack[t.sp++] = make_int2(ref[k], __float_as_int(key[k]));
+        } else {
+          errbits |= kErrStackOverflow;
+        }
+        t.node = ref[0];
+      } else {
+        pop();
+      }
+      // postpone the first leaf found and keep descending from the stack
+      if (t.node < 0 && t.node != kTravDone && leaf == 0) {
+        leaf = t.node;
+        pop();
+      }
+      if (!__any_sync(__activemask(), leaf == 0)) break;
+    }
+    // ---- leaves
+    for (;;) {
+      int code = 0;
+      if (leaf < 0) {
+        code = ~leaf;
+        leaf = 0;
+      } else if (t.node < 0 && t.node != kTravDone) {
+        code = ~t.node;
+        pop();
+      } else {
+        break;
+      }
+      const int first = code >> 4;
+      const int cnt = (code & 15) + 1;
+      if (kCount) tc->tris += cnt;
+      for (int i = 0; i < cnt; ++i) {
+        const float4 *tp = s.tri + 3 * (size_t)(first + i);
+        const float4 A = __ldg(tp + 0), E1 = __ldg(tp + 1), E2 = __ldg(tp + 2);
+        float u, v;
+        const float tt = tri_hit(t.o, t.d, A, E1, E2, eps, u, v);
+        if (tt > eps && tt < t.h.t) {
+          t.h.t = tt;
+          t.h.u = u;
+          t.h.v = v;
+          t.h.slot = first + i;
+          t.tcull = fminf(t.tcull, cull_bound(tt));
+        }
+      }
+    }
+    if (t.node == kTravDone && leaf == 0) return true;
+  }
+  return t.node == kTravDone && leaf == 0;
+}
+
 // ---- quantized wide nodes (layout ids 5: 4 children in 64 B, 9: 8 children in 96 B)
 // float4 0 = (origin.xyz, biased scale exponents x, y, z and the child count as
 // bytes); then the child refs; then the child boxes as bytes q per plane
@@ -478,7 +582,11 @@ TS_D bool trav_advance(const DevScene &s, Traversal &t, int2 *stack, float eps, 
   if (W == 2) return trav_steps<kCount>(s, t, stack, eps, budget, errbits, tc);
   if (W == 3) return trav_steps_spec<kCount>(s, t, stack, eps, budget, errbits, tc);
   if (W == 5 || W == 9) return trav_steps_q<W, kCount>(s, t, stack, eps, budget, errbits, tc);
+#ifdef TS_WIDE_SPECULATIVE
+  return trav_steps_wide_spec<W, kCount>(s, t, stack, eps, budget, errbits, tc);
+#else
   return trav_steps_wide<W, kCount>(s, t, stack, eps, budget, errbits, tc);
+#endif
 }
 
 template <int W>
