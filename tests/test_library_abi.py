@@ -131,3 +131,22 @@ def test_integration_doc_structs_match_the_header():
                         and call.args:
                     assert len(call.args) == len(st._fields_), (node.name, len(call.args))
     assert found >= 1
+
+
+def test_new_entry_points_validate_arguments_without_a_gpu():
+    """ts_create_view, ts_record_paths and ts_set_loop_iteration_limit reject
+    null handles before touching a device."""
+    lib = _lib.load()
+    out = ctypes.c_void_p()
+    cfg = sb.RenderConfig(width=4, height=4).to_c()
+    assert lib.ts_create_view(None, ctypes.byref(cfg), ctypes.byref(out)) == 1 and not out.value
+    assert b"null argument" in lib.ts_last_error(None)
+    assert lib.ts_record_paths(None, 0, 4) == 1
+    assert lib.ts_set_loop_iteration_limit(None, 3) == 1
+
+
+def test_batch_config_carries_the_engine_fields():
+    from spectral_b200 import batch
+    names = [n for n, _ in batch.TsBatchConfig._fields_]
+    assert names[-3:] == ["kernel", "queue_capacity", "trace_budget"]
+    assert ctypes.sizeof(batch.TsBatchConfig) == 7 * 4
