@@ -119,6 +119,12 @@ __global__ void __launch_bounds__(kMaxBlock, 4) k_trace(DevScene s, DevConfig c,
   bool exhausted = false;
   Traversal t;
   int2 stack[StackSize<W>::value];
+#ifdef TS_SHORT_STACK
+  // measurement variant: the newest TS_SHORT_STACK entries of each lane's
+  // wide-node stack in shared memory (dynamic, TS_SHORT_STACK x block entries)
+  extern __shared__ int2 short_stack_smem[];
+  ShortStack<TS_SHORT_STACK> sst{short_stack_smem, stack, (int)blockDim.x, (int)threadIdx.x, 0};
+#endif
   ShadowQuery sq;
   ShadowState ss;
   for (;;) {
@@ -162,7 +168,16 @@ __global__ void __launch_bounds__(kMaxBlock, 4) k_trace(DevScene s, DevConfig c,
       }
     }
     if (__ballot_sync(0xffffffffu, item >= 0) == 0) break;
-    if (item >= 0 && trav_advance<W>(s, t, stack, c.eps, budget, eb)) {
+    bool done = false;
+    if (item >= 0) {
+#ifdef TS_SHORT_STACK
+      if constexpr (W == 4 || W == 8) done = trav_steps_wide<W>(s, t, sst, c.eps, budget, eb);
+      else done = trav_advance<W>(s, t, stack, c.eps, budget, eb);
+#else
+      done = trav_advance<W>(s, t, stack, c.eps, budget, eb);
+#endif
+    }
+    if (done) {
       if (item < nsh) {
         if (shadow_segment(s, c, sq, t.h, band, ss)) {
           if (ss.total > 1e-6f) deposit(f, pixel, dep_band, sq.contrib * ss.total, shared);
@@ -183,18 +198,23 @@ template <bool kLoop = false>
 void launch_trace(const DevScene &s, const DevConfig &c, int depth, Film f, const WaveBuffers &w, uint32_t *err,
                   int grid, int block, cudaStream_t st, int budget, int ext_sorted = 0, int shadow_sorted = 0,
                   WaveLoop *L = nullptr) {
+#ifdef TS_SHORT_STACK
+  const size_t smem = (size_t)TS_SHORT_STACK * block * sizeof(int2);
+#else
+  const size_t smem = 0;
+#endif
   if (s.node_width == 9)
-    k_trace<9, kLoop><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget, ext_sorted, shadow_sorted, L);
+    k_trace<9, kLoop><<<grid, block, smem, st>>>(s, c, depth, f, w, err, budget, ext_sorted, shadow_sorted, L);
   else if (s.node_width == 5)
-    k_trace<5, kLoop><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget, ext_sorted, shadow_sorted, L);
+    k_trace<5, kLoop><<<grid, block, smem, st>>>(s, c, depth, f, w, err, budget, ext_sorted, shadow_sorted, L);
   else if (s.node_width == 8)
-    k_trace<8, kLoop><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget, ext_sorted, shadow_sorted, L);
+    k_trace<8, kLoop><<<grid, block, smem, st>>>(s, c, depth, f, w, err, budget, ext_sorted, shadow_sorted, L);
   else if (s.node_width == 4)
-    k_trace<4, kLoop><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget, ext_sorted, shadow_sorted, L);
+    k_trace<4, kLoop><<<grid, block, smem, st>>>(s, c, depth, f, w, err, budget, ext_sorted, shadow_sorted, L);
   else if (c.speculative)
-    k_trace<3, kLoop><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget, ext_sorted, shadow_sorted, L);
+    k_trace<3, kLoop><<<grid, block, smem, st>>>(s, c, depth, f, w, err, budget, ext_sorted, shadow_sorted, L);
   else
-    k_trace<2, kLoop><<<grid, block, 0, st>>>(s, c, depth, f, w, err, budget, ext_sorted, shadow_sorted, L);
+    k_trace<2, kLoop><<<grid, block, smem, st>>>(s, c, depth, f, w, err, budget, ext_sorted, shadow_sorted, L);
 }
 
 // ---- queue sorting ------------------------------------------------------

@@ -280,11 +280,51 @@ TS_D void sort_children(float *k, int *r) {
   }
 }
 
+// Traversal stacks of (node, entry-distance bits): a plain per-lane array
+// (local memory, kept in L1), or a short stack whose newest S entries of each
+// lane sit in a shared-memory column laid out [entry][thread] -- consecutive
+// threads, consecutive 8-byte words, so a warp touches no bank twice at any
+// mix of depths -- with older entries spilled to the lane's local array.
+TS_D void spush(int2 *st, Traversal &t, int2 e) { st[t.sp++] = e; }
+TS_D int2 spop(int2 *st, Traversal &t) { return st[--t.sp]; }
+
+template <int S>
+struct ShortStack {
+  static_assert((S & (S - 1)) == 0, "ring size must be a power of two");
+  int2 *sm;    // shared: [S][stride] entries
+  int2 *loc;   // local: entries by absolute position (the older ones)
+  int stride;  // threads per block
+  int lane;    // this thread's column
+  int ins;     // top entries held in shared memory (0 after trav_begin)
+};
+template <int S>
+TS_D void spush(ShortStack<S> &st, Traversal &t, int2 e) {
+  const int pos = t.sp;
+  if (st.ins > pos) st.ins = pos;  // a new traversal (trav_begin) emptied the stack
+  if (st.ins == S) {  // ring full: the oldest shared entry moves to local memory
+    const int old = pos - S;
+    st.loc[old] = st.sm[(old & (S - 1)) * st.stride + st.lane];
+    --st.ins;
+  }
+  st.sm[(pos & (S - 1)) * st.stride + st.lane] = e;
+  ++st.ins;
+  ++t.sp;
+}
+template <int S>
+TS_D int2 spop(ShortStack<S> &st, Traversal &t) {
+  const int pos = --t.sp;
+  if (st.ins > 0) {
+    --st.ins;
+    return st.sm[(pos & (S - 1)) * st.stride + st.lane];
+  }
+  return st.loc[pos];
+}
+
 // Same contract as trav_steps, for the wide layout: the children a node's
 // ray enters are sorted by entry distance; the nearest is visited next and
 // the others are pushed (farthest first) with their entry distances.
-template <int W, bool kCount = false>
-TS_D bool trav_steps_wide(const DevScene &s, Traversal &t, int2 *stack, float eps, int budget, uint32_t &errbits,
+template <int W, bool kCount = false, class Stk = int2 *>
+TS_D bool trav_steps_wide(const DevScene &s, Traversal &t, Stk &stack, float eps, int budget, uint32_t &errbits,
                           TraceCount *tc = nullptr) {
   constexpr int P = W / 4;  // float4s per row
   for (int it = 0; it < budget; ++it) {
@@ -321,7 +361,7 @@ TS_D bool trav_steps_wide(const DevScene &s, Traversal &t, int2 *stack, float ep
         if (t.sp + nh - 1 <= kWideStack) {
 #pragma unroll
           for (int k = W - 1; k >= 1; --k)
-            if (k < nh) stack[t.sp++] = make_int2(ref[k], __float_as_int(key[k]));
+            if (k < nh) spush(stack, t, make_int2(ref[k], __float_as_int(key[k])));
         } else {
           errbits |= kErrStackOverflow;
         }
@@ -352,7 +392,7 @@ TS_D bool trav_steps_wide(const DevScene &s, Traversal &t, int2 *stack, float ep
         t.node = kTravDone;
         return true;
       }
-      const int2 e = stack[--t.sp];
+      const int2 e = spop(stack, t);
       if (__int_as_float(e.y) <= t.tcull) {
         t.node = e.x;
         break;
