@@ -49,6 +49,8 @@ def parse():
     p.add_argument("--width", type=int, default=2, choices=[2, 4, 8], help="BVH node width")
     p.add_argument("--quantize", action="store_true", help="4- / 8-wide nodes with 8-bit child boxes (--no-tune)")
     p.add_argument("--traversal", default="default", choices=["default", "speculative"])
+    p.add_argument("--leaf-max", type=int, default=0, help="largest BVH leaf the SAH may choose, 1..16 (--no-tune; 0 = 8)")
+    p.add_argument("--cost-trav", type=float, default=0.0, help="SAH node-visit cost per triangle test (--no-tune; 0 = 1)")
     p.add_argument("--occupancy", type=int, default=0, choices=[0, 8], help="megakernel register budget (--no-tune)")
     p.add_argument("--launch", default="bundle", choices=["bundle", "pass"],
                    help="render each step's 25 passes in one launch (a wavelength bundle) or one launch per pass")
@@ -66,6 +68,11 @@ def parse():
     p.add_argument("--rmse-workloads", default="box,terrain,volume", help="workloads of --workload rmse")
     p.add_argument("--batch-scenes", type=int, default=64, help="scenes of the batched workload (--workload batch)")
     p.add_argument("--batch-target", type=float, default=0.05, help="RMSE target of the batched workload")
+    p.add_argument("--batch-engines", default="kernel,loop,streams",
+                   help="batched engines to run to the target (--workload batch): kernel, loop, streams")
+    p.add_argument("--batch-plain-blocks", type=int, default=0,
+                   help="time the plain arm on this many blocks per scene and scale it by the blocks the batched "
+                        "engines needed (0: run the plain arm to the target too)")
     p.add_argument("--passes", type=int, default=25, help="passes per adjoint launch (--workload adjoint)")
     p.add_argument("--gradcheck-blocks", type=int, default=40, help="blocks per evaluation (--workload gradcheck)")
     p.add_argument("--gradcheck-res", type=int, default=128, help="resolution (--workload gradcheck)")
@@ -82,11 +89,26 @@ def workload(name):
     elif name == "box":
         scene, cfg, ex = configs.box_scene()
         desc = "box: 12-tri box + 2048-tri GGX dielectric sphere + quad light; 256x256, depth 8, 25 bands, 64 spp"
+    elif name == "inverse-target":
+        scene, cfg, ex = configs.volume_scene(width=256, height=256, depth=32)
+        desc = ("inverse-rendering target: the volume scene at 256x256, depth 32, 25 bands, with the hidden "
+                "79 parameters of seed 7 (wall albedos, sigma_a, g, roughnesses)")
     else:
         scene, cfg, ex = configs.volume_scene()
         desc = ("volume: box + 20k-tri HG medium (g 0.7) + fluorescent wall; 512x512, depth 32, 25 bands, "
                 "512 spp")
     return scene, cfg, ex, desc
+
+
+def apply_workload(r, name):
+    """Workload state beyond the scene dictionary: the inverse-rendering target
+    renders the hidden parameters of seed 7 (material table upload)."""
+    if name != "inverse-target":
+        return
+    from spectral_b200 import autodiff, inverse
+    hidden = inverse.Params.from_scene_params(inverse.scene_params(7), "cuda")
+    mat = inverse.material_table(autodiff.material_table(r), hidden, r.config.wavelengths()).float().contiguous()
+    r.update_materials(mat, None)
 
 
 def step_config(cfg, ex, desc, world, num_tris):
@@ -251,6 +273,7 @@ def rmse_leg(name, target, seconds, bundles=True):
                             first_pass=1 << 26, bundles=bundles)
     cfg = best.apply(cfg)
     r = sb.Renderer(scene, cfg, eems=ex["eems"], cmf=ex["cmf"], bvh_params=best.bvh_params())
+    apply_workload(r, name)
     B = cfg.bands
     r.cast_rays_bundle(0, B, pass_idx=0)
     r.clear_pixel_space()
@@ -328,6 +351,7 @@ def plain_seconds(name, blocks, timed_blocks=6):
     cfg.sort_keys = 0
     cfg.trace_budget = 16
     r = sb.Renderer(scene, cfg, eems=ex["eems"], cmf=ex["cmf"], bvh_params={"width": 4})
+    apply_workload(r, name)
     B = cfg.bands
     for k in range(B):
         r.cast_rays(k, pass_idx=(1 << 26) + k)  # warm-up
@@ -550,8 +574,16 @@ def bench_batch(args):
     triangles, 128^2-512^2, depth 4-16), each rendered to a relative XYZ RMSE
     target, one scene at a time with one launch per pass (plain) and all
     scenes together: by the batched persistent kernel replayed as a CUDA graph,
-    and by the stream engine (each scene's block one regenerating wavefront
-    loop launch, scenes overlapping on a pool of streams)."""
+    by the batch loop (every scene's block in one regenerating wavefront loop
+    per step, one CUDA graph), and by the stream engine (each scene's block one
+    loop launch, scenes overlapping on a pool of streams).
+
+    Every arm renders the same paths (the same pass indices of the same random
+    streams) and checks its estimate on the same schedule, so each arm needs
+    the same blocks per scene.  With --batch-plain-blocks N the plain arm is
+    timed on N blocks of every scene and its time to the target is the sum over
+    scenes of (blocks the batched engines needed) x (measured seconds per
+    block): a measured per-scene throughput, not an extrapolated error."""
     import torch
     import spectral_b200 as sb
     from spectral_b200 import batch as sbatch
@@ -564,17 +596,31 @@ def bench_batch(args):
     build_s = time.time() - t0
     B = rs[0].config.bands
     target = args.batch_target
+    engines_wanted = [e for e in args.batch_engines.split(",") if e]
+    assert engines_wanted and all(e in ("kernel", "loop", "streams") for e in engines_wanted), args.batch_engines
+
+    def plain_block(r, nb):
+        for k in range(B):
+            r.cast_rays(k, pass_idx=nb * B + k)
+        r.average_and_reset_block(nb + 1)
+
+    plain, plain_block_s = [], []
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    plain = []
     for r in rs:
         r.clear_pixel_space()
+        if args.batch_plain_blocks > 0:
+            torch.cuda.synchronize()
+            ts0 = time.perf_counter()
+            for nb in range(args.batch_plain_blocks):
+                plain_block(r, nb)
+            torch.cuda.synchronize()
+            plain_block_s.append((time.perf_counter() - ts0) / args.batch_plain_blocks)
+            continue
         nb, due = 0, 2
         while True:
-            for k in range(B):
-                r.cast_rays(k, pass_idx=nb * B + k)
+            plain_block(r, nb)
             nb += 1
-            r.average_and_reset_block(nb)
             if nb >= due:  # the same checking policy as Batch.render_to_rmse
                 e = sbatch.relative_rmse_estimate(r, nb)
                 if e <= target:
@@ -584,53 +630,50 @@ def bench_batch(args):
     torch.cuda.synchronize()
     tp = time.perf_counter() - t0
     from spectral_b200 import autotune
-    t0 = time.time()
-    (bs, bpsm, occ), _ = autotune.tune_batch(rs, steps=1)
-    tune_s = time.time() - t0
-    with sbatch.Batch(rs, block_size=bs, blocks_per_sm=bpsm, occupancy=occ, use_graph=True) as b:
-        b.reset()
-        b.step()
-        b.reset()
-        blocks, tb = b.render_to_rmse(target=target)
-        bits = b.check()
-    paths = sum(int(n) * B * r.config.width * r.config.height for n, r in zip(blocks, rs))
-    # the same scenes through the batch loop: every scene's block in one regenerating
-    # wavefront loop per step, the step one CUDA graph
-    with sbatch.Batch(rs, kernel="wavefront", use_graph=True) as bl:
-        bl.reset()
-        bl.step()
-        bl.reset()
-        blocks_l, tl = bl.render_to_rmse(target=target)
-        bits |= bl.check()
-    paths_l = sum(int(n) * B * r.config.width * r.config.height for n, r in zip(blocks_l, rs))
-    # the same scenes through the stream engine: each scene's block one regenerating
-    # wavefront loop launch, the scenes spread over a pool of streams
-    with sbatch.StreamBatch(rs, streams=8) as sbt:
-        sbt.reset()
-        sbt.step()
-        sbt.reset()
-        blocks_s, ts = sbt.render_to_rmse(target=target)
-        bits |= sbt.check()
-    paths_s = sum(int(n) * B * r.config.width * r.config.height for n, r in zip(blocks_s, rs))
-    engines = {"kernel": tb, "loop": tl, "streams": ts}
-    best = min(engines, key=engines.get)
-    line = {"metric": f"seconds to {target:.0%} relative XYZ RMSE, all scenes", "value": engines[best], "unit": "s",
-            "higher_is_better": False, "n_gpus": 1, "impl": "ours", "data": "synthetic (seeded procedural scenes)",
+    results, bits, tune = {}, 0, None
+    for name in engines_wanted:
+        if name == "kernel":
+            t0 = time.time()
+            (bs, bpsm, occ), _ = autotune.tune_batch(rs, steps=1)
+            tune = {"block_size": bs, "blocks_per_sm": bpsm, "occupancy": occ, "seconds": time.time() - t0}
+            eng = sbatch.Batch(rs, block_size=bs, blocks_per_sm=bpsm, occupancy=occ, use_graph=True)
+            what = "all scenes in one persistent megakernel launch per step (CUDA graph)"
+        elif name == "loop":
+            eng = sbatch.Batch(rs, kernel="wavefront", use_graph=True)
+            what = "all scenes in one regenerating wavefront loop per step (one CUDA graph)"
+        else:
+            eng = sbatch.StreamBatch(rs, streams=8)
+            what = "per scene one regenerating wavefront loop per block, 8 streams"
+        with eng as b:
+            b.reset()
+            b.step()
+            b.reset()
+            blocks, secs = b.render_to_rmse(target=target)
+            bits |= b.check()
+        paths = sum(int(n) * B * r.config.width * r.config.height for n, r in zip(blocks, rs))
+        results[name] = {"seconds": secs, "mpaths_per_s": paths / secs / 1e6, "blocks": [int(x) for x in blocks],
+                         "what": what}
+    if args.batch_plain_blocks > 0:
+        need = results[engines_wanted[0]]["blocks"]
+        tp = sum(n * t for n, t in zip(need, plain_block_s))
+        plain = need
+    for v in results.values():
+        v["speedup"] = tp / v["seconds"]
+    best = min(results, key=lambda k: results[k]["seconds"])
+    line = {"metric": f"seconds to {target:.0%} relative XYZ RMSE, all scenes", "value": results[best]["seconds"],
+            "unit": "s", "higher_is_better": False, "n_gpus": 1, "impl": "ours",
+            "data": "synthetic (seeded procedural scenes)",
             "config": {"workload": f"{len(rs)} scenes of seeds 100-{99 + len(rs)}: box / terrain / volume, "
                                    "1k-500k triangles, 128^2-512^2, depth 4-16",
                        "scene_build_seconds": build_s},
-            "plain_seconds": tp, "batched_seconds": engines[best], "speedup": tp / engines[best], "engine": best,
-            "loop_engine": {"seconds": tl, "speedup": tp / tl, "mpaths_per_s": paths_l / tl / 1e6,
-                            "blocks": [int(x) for x in blocks_l],
-                            "what": "all scenes in one regenerating wavefront loop per step (one CUDA graph)"},
-            "kernel_engine": {"seconds": tb, "speedup": tp / tb, "mpaths_per_s": paths / tb / 1e6,
-                              "what": "all scenes in one persistent megakernel launch per step (CUDA graph)"},
-            "stream_engine": {"seconds": ts, "speedup": tp / ts, "mpaths_per_s": paths_s / ts / 1e6,
-                              "blocks": [int(x) for x in blocks_s], "streams": 8,
-                              "what": "per scene one regenerating wavefront loop per block, 8 streams"},
-            "batch_autotune": {"block_size": bs, "blocks_per_sm": bpsm, "occupancy": occ, "seconds": tune_s},
-            "blocks_plain": plain, "blocks_batched": [int(x) for x in blocks],
-            "batched_mpaths_per_s": paths / tb / 1e6, "device_error_bits": bits,
+            "plain_seconds": tp, "batched_seconds": results[best]["seconds"],
+            "speedup": tp / results[best]["seconds"], "engine": best,
+            "plain": {"what": "one scene at a time, one megakernel launch per pass (the reference's cadence)",
+                      "timed": ("%d blocks per scene, scaled by the blocks the engines needed" % args.batch_plain_blocks
+                                if args.batch_plain_blocks > 0 else "run to the target"),
+                      "blocks": [int(x) for x in plain],
+                      "seconds_per_block": plain_block_s or None},
+            "engines": results, "batch_autotune": tune, "device_error_bits": bits,
             "scenes": [{"res": r.config.width, "tris": r.compiled.num_tris, "depth": r.config.max_path_length}
                        for r in rs]}
     for r in rs:
@@ -740,7 +783,8 @@ def bench_ours(args):
                                  f"/o{c.occupancy}/q{c.queue_capacity}/t{c.trace_budget}": round(ms, 4)
                                  for c, ms in table}}
     comp = sb.compile_scene(scene, cfg.bands, eems=ex["eems"], cmf=ex["cmf"])
-    bvh = sb._lib.build_bvh_host(comp.tris["v0"], comp.tris["v1"], comp.tris["v2"])
+    bvh = sb._lib.build_bvh_host(comp.tris["v0"], comp.tris["v1"], comp.tris["v2"], leaf_max=args.leaf_max,
+                                 cost_trav=args.cost_trav)
     r = sb.Renderer(scene, cfg, eems=ex["eems"], cmf=ex["cmf"], bvh=bvh,
                     bvh_params={"width": args.width, "quantize": args.quantize})
     B = cfg.bands
@@ -860,6 +904,7 @@ def bench_ours(args):
             "config": step_config(cfg, ex, desc, world, comp.num_tris),
             "launch": {"kernel": args.kernel, "bvh_width": args.width, "bvh_quantized": bool(args.quantize),
                        "node_bytes": node_bytes, "traversal": args.traversal,
+                       "bvh_leaf_max": args.leaf_max or 8, "bvh_cost_trav": args.cost_trav or 1.0,
                        "occupancy": args.occupancy, "queue_capacity": cfg.queue_capacity,
                        "block_size": cfg.block_size, "trace_budget": cfg.trace_budget, "launches": launches},
             "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": 36,
