@@ -3,7 +3,11 @@
 The box scene with the HG medium and the fluorescent back wall, with 79
 unknowns: the per-band albedos of the left and right walls (2 x 25), the
 medium's per-band absorption sigma_a (25), its HG anisotropy g, and the GGX
-roughnesses of the fluorescent back wall and the left and right walls (3).
+roughnesses of the fluorescent back wall and the left and right walls (3):
+under the reference's surface model (main.py:1384-1412) a wall of roughness
+above 0.008 carries a GGX lobe with the Fresnel term of its n = 1.5 coating
+over an Oren-Nayar diffuse term of sigma = roughness * pi / 2, so each
+roughness moves both.
 The medium's boundary stays a smooth dielectric: under the reference's
 estimator a rough dielectric boundary transmits nothing (its Smith term
 clamps the refracted cosine to zero), which would hide the medium.  A target image is
