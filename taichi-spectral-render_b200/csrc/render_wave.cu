@@ -169,6 +169,15 @@ __global__ void __launch_bounds__(kMaxBlock, 4) k_trace(DevScene s, DevConfig c,
     }
     if (__ballot_sync(0xffffffffu, item >= 0) == 0) break;
     bool done = false;
+#if defined(TS_IDLE_REFILL)
+    // measurement variant: the warp steps its rays one traversal step at a
+    // time and refills as soon as TS_IDLE_REFILL lanes could take new work
+    // (dynamic fetch), within the same bound of `budget` steps
+    for (int st = 0; st < budget; ++st) {
+      if (item >= 0 && !done) done = trav_advance<W>(s, t, stack, c.eps, 1, eb);
+      if (__popc(__ballot_sync(0xffffffffu, done || (item < 0 && !exhausted))) >= TS_IDLE_REFILL) break;
+    }
+#else
     if (item >= 0) {
 #ifdef TS_SHORT_STACK
       if constexpr (W == 4 || W == 8) done = trav_steps_wide<W>(s, t, sst, c.eps, budget, eb);
@@ -177,6 +186,7 @@ __global__ void __launch_bounds__(kMaxBlock, 4) k_trace(DevScene s, DevConfig c,
       done = trav_advance<W>(s, t, stack, c.eps, budget, eb);
 #endif
     }
+#endif
     if (done) {
       if (item < nsh) {
         if (shadow_segment(s, c, sq, t.h, band, ss)) {
