@@ -393,13 +393,18 @@ def bench_gradcheck(args):
         bits = r.check_device()
     secs = time.perf_counter() - t0
     rel = np.array([abs(x["adjoint"] - x["fd"]) / max(abs(x["fd"]), 1e-300) for x in rows])
-    z = np.array([(x["adjoint"] - x["fd"]) / max(x["fd_sem"], 1e-300) for x in rows])
+    # both sides are Monte Carlo estimates on the same paths; their errors are
+    # positively correlated, so the combined error below is an upper bound
+    sem = np.array([np.hypot(x["fd_sem"], np.nan_to_num(x["adjoint_sem"])) for x in rows])
+    z = np.array([(x["adjoint"] - x["fd"]) / max(e, 1e-300) for x, e in zip(rows, sem)])
     noise = np.array([x["fd_sem"] / max(abs(x["fd"]), 1e-300) for x in rows])
+    adj_noise = np.array([x["adjoint_sem"] / max(abs(x["adjoint"]), 1e-300) for x in rows])
     groups = {}
     for name in ("albedo_left", "albedo_right", "sigma_a", "g", "roughness"):
         idx = [i for i, x in enumerate(rows) if x["name"] == name]
         groups[name] = {"parameters": len(idx), "within_2pct": int((rel[idx] <= 0.02).sum()),
                         "max_rel_err": float(rel[idx].max()), "median_fd_rel_sem": float(np.median(noise[idx])),
+                        "median_adjoint_rel_sem": float(np.median(adj_noise[idx])),
                         "max_abs_z": float(np.abs(z[idx]).max()),
                         "within_2pct_or_3_sem": int(((rel[idx] <= 0.02) | (np.abs(z[idx]) <= 3)).sum())}
     print(json.dumps({"metric": "adjoint vs central finite differences", "parameters": len(rows),
@@ -407,6 +412,7 @@ def bench_gradcheck(args):
                       "within_2pct": int((rel <= 0.02).sum()), "max_rel_err": float(rel.max()),
                       "median_rel_err": float(np.median(rel)), "max_abs_z": float(np.abs(z).max()),
                       "max_fd_rel_sem": float(noise.max()), "h": "1e-3 relative to each parameter",
+                      "z": "(adjoint - fd) / hypot(fd_sem, adjoint_sem); adjoint_sem from 10 groups of blocks",
                       "blocks": args.gradcheck_blocks,
                       "config": {"workload": f"volume scene (HG medium g 0.7, fluorescent wall) {res}x{res}, depth 32, "
                                              "25 bands; 79 parameters of seed 8"},

@@ -149,7 +149,7 @@ def parameter_error(p, q):
 NAMES = ("albedo_left", "albedo_right", "sigma_a", "g", "roughness")
 
 
-def gradient_check(renderer, params, h=1e-3, blocks=40, first_pass=1 << 22, seed=0):
+def gradient_check(renderer, params, h=1e-3, blocks=40, first_pass=1 << 22, seed=0, groups=10):
     """The adjoint against central finite differences, parameter by parameter.
 
     The functional is L(theta) = sum(w * film(theta)) with a fixed random
@@ -161,8 +161,12 @@ def gradient_check(renderer, params, h=1e-3, blocks=40, first_pass=1 << 22, seed
     of the 79 physical parameters (albedos, sigma_a [1/m], g, roughnesses:
     step h * |value|, so that no step leaves a parameter's domain -- sigma_a
     spans orders of magnitude over the bands); the per-block differences give
-    the standard error of the estimate.  Returns a list of dicts (name, index,
-    value, step, adjoint, fd, fd_sem)."""
+    the standard error of the estimate.  The adjoint is itself a Monte Carlo
+    estimate (its score terms add variance of their own): it is computed over
+    ``groups`` equal runs of consecutive blocks, whose spread gives its
+    standard error, and its mean is the gradient over all ``blocks``.
+    Returns a list of dicts (name, index, value, step, adjoint, adjoint_sem,
+    fd, fd_sem)."""
     r = renderer
     B = r.config.bands
     base = autodiff.material_table(r)
@@ -171,11 +175,19 @@ def gradient_check(renderer, params, h=1e-3, blocks=40, first_pass=1 << 22, seed
     gen = torch.Generator(device=r.device)
     gen.manual_seed(seed)
     w = torch.rand((B, r.config.height, r.config.width), dtype=torch.float64, device=r.device, generator=gen)
-    leaves = {n: getattr(params, n).detach().clone().to(torch.float64).requires_grad_(True) for n in NAMES}
-    film = autodiff.render_film(r, material_table(base, Params(**leaves), lam), eem, first_pass=first_pass,
-                                num_blocks=blocks)
-    (film * w).sum().backward()
+    if groups < 1 or blocks % groups:
+        groups = 1
+    per = blocks // groups
+    grads = {n: [] for n in NAMES}
+    for g in range(groups):
+        leaves = {n: getattr(params, n).detach().clone().to(torch.float64).requires_grad_(True) for n in NAMES}
+        film = autodiff.render_film(r, material_table(base, Params(**leaves), lam), eem,
+                                    first_pass=first_pass + g * per * B, num_blocks=per)
+        (film * w).sum().backward()
+        for n in NAMES:
+            grads[n].append(leaves[n].grad.detach().reshape(-1))
     r.record_paths(0, 0)
+    gstack = {n: torch.stack(grads[n]) for n in NAMES}  # [groups, count]
 
     def per_block(p):
         r.update_materials(material_table(base, p, lam).float().contiguous(), None)
@@ -191,7 +203,9 @@ def gradient_check(renderer, params, h=1e-3, blocks=40, first_pass=1 << 22, seed
     for name in NAMES:
         val = getattr(params, name).detach().to(torch.float64)
         flat = val.reshape(-1)
-        grad = leaves[name].grad.reshape(-1)
+        grad = gstack[name].mean(0)
+        grad_sem = (gstack[name].std(0, unbiased=True) / groups ** 0.5 if groups > 1
+                    else torch.full_like(grad, float("nan")))
         for i in range(flat.numel()):
             lo = {n: getattr(params, n).detach().to(torch.float64) for n in NAMES}
             hi = dict(lo)
@@ -202,7 +216,8 @@ def gradient_check(renderer, params, h=1e-3, blocks=40, first_pass=1 << 22, seed
             lo[name] = (flat - dp).reshape(val.shape)
             d = (per_block(Params(**hi)) - per_block(Params(**lo))) / (2.0 * step)
             rows.append({"name": name, "index": i, "value": float(flat[i]), "step": step, "adjoint": float(grad[i]),
-                         "fd": float(d.mean()), "fd_sem": float(d.std(ddof=1) / np.sqrt(blocks))})
+                         "adjoint_sem": float(grad_sem[i]), "fd": float(d.mean()),
+                         "fd_sem": float(d.std(ddof=1) / np.sqrt(blocks))})
     # leave the renderer with the unperturbed tables
     r.update_materials(material_table(base, params, lam).float().contiguous(), None)
     return rows
