@@ -922,8 +922,8 @@ def bench_ours(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
                          "traffic": None if traffic is None else traffic * B,
-                         "traffic_per": "step (one launch of the timed configuration: DRAM bytes per pass from an "
-                                        "ncu capture x 25 passes)",
+                         "traffic_per": "step (one 25-pass launch): DRAM bytes per pass of the committed ncu capture "
+                                        "(profiles/traffic.json, its source says which case) x 25 passes",
                          "kernel": kernel_name, "bytes_per_path": bytes_per_path,
                          "bytes_per_launch": bytes_per_path * paths_per_step, "peak_source": peak_src,
                          "work_per_path": {k: v / work["paths"] for k, v in work.items() if k != "paths"}},
