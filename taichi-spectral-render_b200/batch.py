@@ -119,14 +119,14 @@ class Batch:
     def wait(self, i):
         """Make the current stream wait for scene i's last step (one stream here: nothing to do)."""
 
-    def render_to_rmse(self, target=0.01, max_blocks=100000, min_blocks=2, estimator=None):
+    def render_to_rmse(self, target=0.01, max_blocks=100000, min_blocks=2, estimator=None, max_seconds=None):
         """Steps until every scene's relative XYZ RMSE estimate is <= target.
 
         A scene's estimate is evaluated only when it is due: after an estimate e
         at n blocks the next check comes at the block count where 1/sqrt(n)
         scaling predicts the target (``next_check``).  Returns per-scene blocks
         rendered and the wall time (device-synchronised)."""
-        return render_to_rmse(self, target, max_blocks, min_blocks, estimator)
+        return render_to_rmse(self, target, max_blocks, min_blocks, estimator, max_seconds)
 
 
 class StreamBatch:
@@ -214,20 +214,23 @@ class StreamBatch:
             bits |= r.check_device()
         return bits
 
-    def render_to_rmse(self, target=0.01, max_blocks=100000, min_blocks=2, estimator=None):
+    def render_to_rmse(self, target=0.01, max_blocks=100000, min_blocks=2, estimator=None, max_seconds=None):
         """As ``Batch.render_to_rmse``."""
-        return render_to_rmse(self, target, max_blocks, min_blocks, estimator)
+        return render_to_rmse(self, target, max_blocks, min_blocks, estimator, max_seconds)
 
 
-def render_to_rmse(batch, target=0.01, max_blocks=100000, min_blocks=2, estimator=None):
+def render_to_rmse(batch, target=0.01, max_blocks=100000, min_blocks=2, estimator=None, max_seconds=None):
     """Steps ``batch`` until every scene's relative XYZ RMSE estimate is <= target
-    (checks when due, ``next_check``); returns per-scene blocks and the wall time."""
+    (checks when due, ``next_check``), or until ``max_seconds`` have passed (the
+    step under way completes); returns per-scene blocks and the wall time."""
     import torch
     estimator = estimator or relative_rmse_estimate
     due = np.full(len(batch.renderers), min_blocks, np.int64)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     while batch.active.any():
+        if max_seconds is not None and time.perf_counter() - t0 > max_seconds:
+            break
         batch.step()
         flags = batch.active.copy()
         for i, r in enumerate(batch.renderers):
